@@ -1,0 +1,39 @@
+/*
+ * mr_aha_b200.h -- entry points of the B200 implementation that have no
+ * counterpart in the reference library (its public header has no precision,
+ * solver or accounting API). They extend an mr_op created through the
+ * reference-compatible mr_aha.h.
+ */
+#ifndef MR_AHA_MR_AHA_B200_H
+#define MR_AHA_MR_AHA_B200_H
+
+#include "mr_aha/mr_aha.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Kernel storage formats of an operator. */
+#define MR_B200_KF_COMPLEX64 0 /* 8 bytes per packed element (reference layout)   */
+#define MR_B200_KF_BF16 1      /* bfloat16 (re, im) + one float scale per location */
+#define MR_B200_KF_INT16 2     /* int16 (re, im) block floating point + one float
+                                  scale per location: value = scale * code,
+                                  |code| <= 32767, scale = max |re|,|im| / 32767 */
+
+/* No reference counterpart. Store the operator's kernel in `format` for all
+ * later applies (FFTs and arithmetic stay FP32). keep_complex64 = 0 frees the
+ * complex64 copy (then mr_op_kernel fails with MR_ERR_UNSUPPORTED and the
+ * format cannot be changed again). Synchronous. */
+MR_EXPORT int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_complex64);
+
+/* No reference counterpart. Current kernel format of the operator. */
+MR_EXPORT int mr_b200_op_kernel_format(mr_op op, int *format);
+
+/* No reference counterpart. Number of kernels one mr_op_execute launches. */
+MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MR_AHA_MR_AHA_B200_H */

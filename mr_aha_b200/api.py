@@ -1,0 +1,575 @@
+"""Array-level interface, a drop-in for the reference's ``python/mr_aha/api.py``.
+
+Same functions, argument meanings, shapes and errors as the reference binding
+(``make_config`` ``api.py:211-324``, ``calc_mask`` ``:393-447``,
+``calc_toep`` ``:556-639``, ``aha_toeplitz`` ``:642-701``, ``AhAOp`` /
+``create_op`` ``:745-1255``). Arrays are CUDA device arrays: a
+``torch.Tensor`` on a CUDA device, or any object exposing
+``__cuda_array_interface__`` (CuPy, Numba, ...). Shapes are row-major, i.e.
+the column-major shapes of the C API reversed:
+
+============================  =======================================
+column-major (C API)          row-major (this module)
+============================  =======================================
+``x[Nx, Ny, Nz, L]``          ``x[L, Nz, Ny, Nx]``
+``SEs[Nx, Ny, Nz, Nc]``       ``SEs[Nc, Nz, Ny, Nx]``
+``phi2_toep[Mx, My, Mz, T]``  ``phi2_toep[T, Mz, My, Mx]``
+``phi2[Ntrajs, Nkz, L, L]``   ``phi2[L, L, Nkz, Ntrajs]`` (stack)
+``traj[Ntrajs, Nkx, ndim]``   ``traj[ndim, Nkx, Ntrajs]``
+============================  =======================================
+
+``complex64`` for the data arrays, ``float32`` for ``traj``, ``int64`` for
+``mask``; every array C-contiguous. The Gram blocks multiply the rank row
+vector from the right, ``v <- v Phi2`` (``include/mr_aha/mr_aha.h:33-62`` of
+the reference).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import numbers
+from typing import Optional, Sequence
+
+from ._lib import (
+    DEFAULT_MASK_RADIUS,
+    KERNEL_FORMATS,
+    OP_ALL_DEVICES,
+    OP_SHARE_PRIMARY,
+    OP_TOEP_SOURCES,
+    MRConfig,
+    MRError,
+    MROpInfo,
+    MROpInputs,
+    MROpOptions,
+    OpMethod,
+    ToepDist,
+    TrajType,
+    Triangulation,
+    backend,
+    check,
+    lib,
+)
+
+__all__ = [
+    "DEFAULT_MASK_RADIUS", "MRConfig", "MRError", "TrajType", "Triangulation",
+    "make_config", "num_tri", "phi2_toep_shape", "calc_mask", "calc_toep",
+    "calc_toep_from_psf", "aha_toeplitz", "AhAPlan", "AhAOp", "create_op",
+]
+
+_DTYPES = {"complex64": 8, "float32": 4, "int64": 8}
+
+
+def _torch():
+    import torch  # noqa: PLC0415
+    return torch
+
+
+def _is_torch(a) -> bool:
+    t = type(a)
+    return t.__module__.startswith("torch") and hasattr(a, "data_ptr")
+
+
+def _ptr(array, name: str, dtype: str, allow_none: bool = False):
+    """Validate a device array and return its device pointer.
+
+    Raises ``TypeError`` for host arrays or a wrong dtype and ``ValueError``
+    for non-contiguous arrays, like the reference's ``_ptr`` (``api.py:155-209``).
+    """
+    if array is None:
+        if allow_none:
+            return None
+        raise TypeError(f"{name} must not be None")
+    if _is_torch(array):
+        torch = _torch()
+        want = {"complex64": torch.complex64, "float32": torch.float32,
+                "int64": torch.int64}[dtype]
+        if not array.is_cuda:
+            raise TypeError(f"{name} must be a CUDA tensor for the {backend()} backend, "
+                            f"got a tensor on {array.device}")
+        if array.dtype != want:
+            raise TypeError(f"{name} must have dtype {want}, got {array.dtype}")
+        if not array.is_contiguous():
+            raise ValueError(f"{name} must be C-contiguous; call .contiguous() first")
+        return int(array.data_ptr()) or None
+    cai = getattr(array, "__cuda_array_interface__", None)
+    if cai is None:
+        raise TypeError(f"{name} must be a CUDA device array (torch.Tensor on a CUDA device "
+                        f"or __cuda_array_interface__), got {type(array).__name__}")
+    import numpy as np  # noqa: PLC0415
+    if np.dtype(cai["typestr"]) != np.dtype(dtype):
+        raise TypeError(f"{name} must have dtype {dtype}, got {np.dtype(cai['typestr'])}")
+    strides = cai.get("strides")
+    if strides is not None:
+        exp, acc = [], np.dtype(dtype).itemsize
+        for n in reversed(cai["shape"]):
+            exp.append(acc)
+            acc *= n
+        if tuple(reversed(exp)) != tuple(strides):
+            raise ValueError(f"{name} must be C-contiguous")
+    return int(cai["data"][0]) or None
+
+
+def _size(array) -> int:
+    if _is_torch(array):
+        return int(array.numel())
+    n = 1
+    for s in array.__cuda_array_interface__["shape"]:
+        n *= int(s)
+    return n
+
+
+def _check_size(array, expected: int, name: str) -> None:
+    if _size(array) != expected:
+        raise ValueError(
+            f"{name} has {_size(array)} elements but {expected} were expected "
+            f"(remember that Python shapes are the reverse of the column-major shapes "
+            f"in the documentation)")
+
+
+def _device_of(*arrays):
+    for a in arrays:
+        if a is not None and _is_torch(a):
+            return a.device
+    torch = _torch()
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _empty(shape, dtype: str, device):
+    torch = _torch()
+    td = {"complex64": torch.complex64, "int64": torch.int64, "float32": torch.float32}[dtype]
+    return torch.empty(tuple(shape), dtype=td, device=device)
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream or None
+    for attr in ("cuda_stream", "ptr"):
+        v = getattr(stream, attr, None)
+        if v is not None:
+            return int(v) or None
+    raise TypeError("stream must be None, an int handle, a torch.cuda.Stream or expose .ptr")
+
+
+def make_config(traj_type, n_dim: Sequence[int], L: int, *,
+                phi2_dim: Optional[Sequence[int]] = None, triangulation="lower",
+                is_masked: bool = False, num_masked: int = 0, n_coils: int = 1,
+                eps: float = 1e-6, gpu_device_id: int = -1, stream=None,
+                mem_fraction: float = 0.5, verbose: bool = False,
+                mask_radius: int = DEFAULT_MASK_RADIUS) -> MRConfig:
+    """Build a validated :class:`MRConfig` (reference ``api.py:211-324``).
+
+    ``n_dim`` / ``phi2_dim`` are column-major ``(Nx, Ny[, Nz])``;
+    ``phi2_dim`` defaults to ``2 * n_dim`` except ``Mz = Nz`` for a stack.
+    ``is_masked=True`` with ``num_masked=0`` is accepted (filled in later).
+    """
+    tt = TrajType.parse(traj_type)
+    cfg = MRConfig()
+    check(lib.mr_config_defaults(ctypes.byref(cfg), tt), "mr_config_defaults")
+    n_spatial = cfg.n_spatial
+    n_dim = [int(v) for v in n_dim]
+    if len(n_dim) != n_spatial:
+        raise ValueError(f"n_dim must have {n_spatial} entries for this trajectory type, "
+                         f"got {len(n_dim)}")
+    if phi2_dim is None:
+        phi2_dim = [2 * v for v in n_dim]
+        if tt == TrajType.STACK:
+            phi2_dim[2] = n_dim[2]
+    else:
+        phi2_dim = [int(v) for v in phi2_dim]
+    if len(phi2_dim) != n_spatial:
+        raise ValueError(f"phi2_dim must have {n_spatial} entries, got {len(phi2_dim)}")
+    for i in range(n_spatial):
+        cfg.n_dim[i] = n_dim[i]
+        cfg.phi2_dim[i] = phi2_dim[i]
+    cfg.L = int(L)
+    cfg.triangulation = Triangulation.parse(triangulation)
+    cfg.is_masked = 1 if is_masked else 0
+    cfg.num_masked = int(num_masked)
+    cfg.n_coils = int(n_coils)
+    cfg.eps = float(eps)
+    cfg.gpu_device_id = int(gpu_device_id)
+    cfg.mem_fraction = float(mem_fraction)
+    cfg.verbose = 1 if verbose else 0
+    cfg.mask_radius = int(mask_radius)
+    cfg.stream = _stream_ptr(stream)
+    probe = MRConfig.from_buffer_copy(cfg)
+    if probe.is_masked and probe.num_masked == 0:
+        probe.is_masked = 0
+    check(lib.mr_config_validate(ctypes.byref(probe)), "mr_config_validate")
+    return cfg
+
+
+def num_tri(L: int) -> int:
+    return int(lib.mr_num_tri(int(L)))
+
+
+def phi2_toep_shape(cfg: MRConfig) -> tuple:
+    """Row-major shape of ``phi2_toep``: ``(ntri, num_masked)`` or ``(ntri, [Mz,] My, Mx)``."""
+    ntri = num_tri(cfg.L)
+    if cfg.is_masked:
+        return (ntri, int(cfg.num_masked))
+    dims = [cfg.phi2_dim[i] for i in range(cfg.n_spatial)]
+    return tuple([ntri] + list(reversed(dims)))
+
+
+def _image_shape(cfg: MRConfig) -> tuple:
+    return tuple(reversed([cfg.n_dim[i] for i in range(cfg.n_spatial)]))
+
+
+def _check_traj(cfg: MRConfig, traj):
+    ndim_traj = 3 if cfg.traj_type == TrajType.THREE_D else 2
+    shape = tuple(traj.shape) if _is_torch(traj) else tuple(traj.__cuda_array_interface__["shape"])
+    if len(shape) != 3 or shape[0] != ndim_traj:
+        raise ValueError(f"traj must be shaped (ndim, Nkx, Ntrajs) with ndim = {ndim_traj}, "
+                         f"got {shape}")
+    _, Nkx, Ntrajs = shape
+    return int(Ntrajs), int(Nkx)
+
+
+def calc_mask(cfg: MRConfig, traj, *, radius: Optional[int] = None):
+    """Neighbourhood mask from the trajectory (reference ``api.py:393-447``)."""
+    Ntrajs, Nkx = _check_traj(cfg, traj)
+    c = MRConfig.from_buffer_copy(cfg)
+    if radius is not None:
+        c.mask_radius = int(radius)
+    dev = _device_of(traj)
+    buf = _empty((int(lib.mr_pad_size(ctypes.byref(c))),), "int64", dev)
+    n = ctypes.c_int64(0)
+    check(lib.mr_calc_mask(ctypes.byref(c), _ptr(traj, "traj", "float32"), ctypes.c_int64(Ntrajs),
+                           ctypes.c_int64(Nkx), _ptr(buf, "mask", "int64"), ctypes.byref(n)),
+          "mr_calc_mask")
+    mask = buf[: n.value].clone()
+    del buf
+    return mask
+
+
+def _check_gram(cfg: MRConfig, phi2, traj, mask):
+    Ntrajs, Nkx = _check_traj(cfg, traj)
+    nkz = cfg.phi2_dim[2] if cfg.traj_type == TrajType.STACK else 1
+    _check_size(phi2, cfg.L * cfg.L * nkz * Ntrajs, "phi2")
+    if cfg.is_masked:
+        if mask is None:
+            raise ValueError("cfg.is_masked is set, so a mask is required")
+        if cfg.num_masked == 0:
+            cfg.num_masked = _size(mask)
+            check(lib.mr_config_validate(ctypes.byref(cfg)), "mr_config_validate")
+        elif _size(mask) != int(cfg.num_masked):
+            raise ValueError(f"mask has {_size(mask)} elements but cfg.num_masked is "
+                             f"{cfg.num_masked}")
+    return Ntrajs, Nkx
+
+
+def calc_toep(cfg: MRConfig, phi2, traj, mask=None, out=None, nufft: Optional[str] = None):
+    """Toeplitz kernel ``phi2_toep`` from the Gram blocks (reference ``api.py:556-639``).
+
+    ``nufft`` is accepted for signature compatibility; only ``None`` /
+    ``'library'`` (the on-GPU build) exist in this implementation.
+    """
+    if nufft not in (None, "library"):
+        raise ValueError(f"nufft={nufft!r}: only the library build is available")
+    Ntrajs, Nkx = _check_gram(cfg, phi2, traj, mask)
+    shape = phi2_toep_shape(cfg)
+    expected = int(lib.mr_phi2_toep_size(ctypes.byref(cfg)))
+    if out is None:
+        out = _empty(shape, "complex64", _device_of(phi2, traj))
+    else:
+        _check_size(out, expected, "out")
+    check(lib.mr_calc_toep(ctypes.byref(cfg), _ptr(phi2, "phi2", "complex64"),
+                           _ptr(traj, "traj", "float32"), ctypes.c_int64(Ntrajs),
+                           ctypes.c_int64(Nkx), _ptr(mask, "mask", "int64", allow_none=True),
+                           _ptr(out, "out", "complex64")), "mr_calc_toep")
+    return out
+
+
+def calc_toep_from_psf(cfg: MRConfig, psf, t0: int, out, mask=None):
+    """Finish components ``[t0, t0 + n)`` of ``out`` from centred PSFs
+    ``psf[n, Mz, My, Mx]`` (reference ``mr_calc_toep_from_psf``)."""
+    vol = 1
+    for i in range(3):
+        vol *= cfg.phi2_dim[i]
+    n = _size(psf) // vol
+    check(lib.mr_calc_toep_from_psf(ctypes.byref(cfg), _ptr(psf, "psf", "complex64"),
+                                    ctypes.c_int64(int(t0)), ctypes.c_int64(n),
+                                    _ptr(mask, "mask", "int64", allow_none=True),
+                                    _ptr(out, "out", "complex64")), "mr_calc_toep_from_psf")
+    return out
+
+
+def aha_toeplitz(cfg: MRConfig, x, SEs, phi2_toep, mask=None, out=None):
+    """One-shot Toeplitz ``A^H A x`` (reference ``api.py:642-701``)."""
+    _check_size(x, int(lib.mr_x_size(ctypes.byref(cfg))), "x")
+    _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
+    _check_size(phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "phi2_toep")
+    if cfg.is_masked and mask is None:
+        raise ValueError("cfg.is_masked is set, so a mask is required")
+    if out is None:
+        out = _empty(tuple(x.shape) if _is_torch(x) else x.__cuda_array_interface__["shape"],
+                     "complex64", _device_of(x))
+    else:
+        _check_size(out, _size(x), "out")
+    check(lib.mr_aha_toeplitz(ctypes.byref(cfg), _ptr(x, "x", "complex64"),
+                              _ptr(SEs, "SEs", "complex64"),
+                              _ptr(phi2_toep, "phi2_toep", "complex64"),
+                              _ptr(mask, "mask", "int64", allow_none=True),
+                              _ptr(out, "out", "complex64")), "mr_aha_toeplitz")
+    return out
+
+
+class AhAPlan:
+    """Reusable stateless plan (``mr_aha_plan_create/execute/destroy``)."""
+
+    def __init__(self, cfg: MRConfig):
+        self._cfg = MRConfig.from_buffer_copy(cfg)
+        self._h = ctypes.c_void_p()
+        check(lib.mr_aha_plan_create(ctypes.byref(self._cfg), ctypes.byref(self._h)),
+              "mr_aha_plan_create")
+
+    def execute(self, x, SEs, phi2_toep, mask=None, out=None):
+        if not self._h:
+            raise RuntimeError("this AhAPlan has already been closed")
+        cfg = self._cfg
+        _check_size(x, int(lib.mr_x_size(ctypes.byref(cfg))), "x")
+        _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
+        _check_size(phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "phi2_toep")
+        if out is None:
+            out = _empty(tuple(x.shape), "complex64", _device_of(x))
+        check(lib.mr_aha_plan_execute(self._h, _ptr(x, "x", "complex64"),
+                                      _ptr(SEs, "SEs", "complex64"),
+                                      _ptr(phi2_toep, "phi2_toep", "complex64"),
+                                      _ptr(mask, "mask", "int64", allow_none=True),
+                                      _ptr(out, "out", "complex64")), "mr_aha_plan_execute")
+        return out
+
+    __call__ = execute
+
+    def close(self):
+        if self._h:
+            lib.mr_aha_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+
+def _devices_arg(devices):
+    if devices is None:
+        return None, 0
+    if isinstance(devices, str):
+        if devices.lower() != "all":
+            raise ValueError(f"devices must be None, 'all', an int or a list; got {devices!r}")
+        return None, OP_ALL_DEVICES
+    if isinstance(devices, numbers.Integral):
+        devices = [devices]
+    devices = [int(d) for d in devices]
+    if not devices:
+        return None, 0
+    return (ctypes.c_int * len(devices))(*devices), len(devices)
+
+
+_NUFFT_OPTS = ("upsampfac", "gpu_method")
+
+
+class AhAOp:
+    """The ``A^H A`` operator (reference ``api.py:745-1235``).
+
+    ``op = create_op(cfg, SEs, phi2, traj)`` builds the Toeplitz kernel on the
+    GPU and a plan; ``op(x)`` applies it on ``cfg.stream``. ``method='nufft'``
+    is rejected by the library (MR_ERR_UNSUPPORTED). One GPU: ``devices``
+    other than the primary are accepted and served by the primary alone.
+    """
+
+    def __init__(self, *args, **kwargs):
+        raise TypeError("AhAOp is created with mr_aha_b200.create_op(cfg, SEs, phi2, traj, ...) "
+                        "(or AhAOp.create_op), not by calling the class")
+
+    @classmethod
+    def create_op(cls, cfg: MRConfig, SEs, phi2, traj, mask=None, *, method: str = "toeplitz",
+                  devices=None, toep_dist: str = "auto", share_primary: bool = True,
+                  nufft_opts: Optional[dict] = None, _phi2_toep=None,
+                  kernel_format: str = "complex64", keep_complex64: bool = True) -> "AhAOp":
+        """Create the operator (``mr_op_create``).
+
+        ``kernel_format`` (``'complex64'``, ``'bf16'`` or ``'int16'``) selects
+        the storage of the kernel read by every apply (no reference
+        counterpart; see ``mr_b200_op_set_kernel_format``).
+        """
+        self = cls.__new__(cls)
+        self._handle = ctypes.c_void_p()
+        self._keep = ()
+        self._method = OpMethod._TO_STR[OpMethod.parse(method)]
+        is_nufft = self._method == "nufft"
+        if is_nufft and cfg.is_masked:
+            raise ValueError("method='nufft' has no kernel to mask; build the configuration "
+                             "with is_masked=False")
+        nufft_opts = dict(nufft_opts or {})
+        if not is_nufft and nufft_opts:
+            raise ValueError("nufft_opts is only used with method='nufft'")
+        unknown = set(nufft_opts) - set(_NUFFT_OPTS)
+        if unknown:
+            raise ValueError(f"unknown nufft_opts {sorted(unknown)}; accepted: {list(_NUFFT_OPTS)}")
+        _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
+        if _phi2_toep is not None and phi2 is None and traj is None and not is_nufft:
+            Ntrajs, Nkx = 0, 0
+            if cfg.is_masked:
+                if mask is None:
+                    raise ValueError("cfg.is_masked is set, so a mask is required")
+                if cfg.num_masked == 0:
+                    cfg.num_masked = _size(mask)
+        else:
+            if phi2 is None or traj is None:
+                raise ValueError("phi2 and traj are required (the operator is built from the "
+                                 "Gram blocks)")
+            Ntrajs, Nkx = _check_gram(cfg, phi2, traj, mask)
+        if _phi2_toep is not None:
+            if is_nufft:
+                raise ValueError("_phi2_toep is only used with method='toeplitz'")
+            _check_size(_phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "_phi2_toep")
+        devs, ndev = _devices_arg(devices)
+        self._cfg = MRConfig.from_buffer_copy(cfg)
+        opt = MROpOptions()
+        check(lib.mr_op_options_defaults(ctypes.byref(opt)), "mr_op_options_defaults")
+        opt.method = OpMethod.parse(method)
+        opt.devices = ctypes.cast(devs, ctypes.POINTER(ctypes.c_int)) if devs else None
+        opt.n_devices = ndev
+        opt.toep_dist = ToepDist.parse(toep_dist)
+        opt.flags = OP_SHARE_PRIMARY if share_primary else 0
+        opt.nufft_upsampfac = float(nufft_opts.get("upsampfac", 0.0))
+        opt.nufft_gpu_method = int(nufft_opts.get("gpu_method", 0))
+        inp = MROpInputs(
+            _ptr(SEs, "SEs", "complex64"),
+            _ptr(phi2, "phi2", "complex64", allow_none=_phi2_toep is not None),
+            _ptr(traj, "traj", "float32", allow_none=_phi2_toep is not None),
+            int(Ntrajs), int(Nkx),
+            _ptr(mask, "mask", "int64", allow_none=True),
+            _ptr(_phi2_toep, "_phi2_toep", "complex64", allow_none=True),
+        )
+        if share_primary:
+            self._keep = (SEs, mask, _phi2_toep)
+        self._device = _device_of(SEs)
+        check(lib.mr_op_create(ctypes.byref(cfg), ctypes.byref(inp), ctypes.byref(opt),
+                               ctypes.byref(self._handle)), "mr_op_create")
+        if kernel_format != "complex64":
+            self.set_kernel_format(kernel_format, keep_complex64=keep_complex64)
+        return self
+
+    @property
+    def config(self) -> MRConfig:
+        return self._cfg
+
+    @property
+    def method(self) -> str:
+        return self._method
+
+    def _check_open(self):
+        if not self._handle:
+            raise RuntimeError("this AhAOp has already been closed")
+
+    def apply(self, x, out=None):
+        """``A^H A x`` (``mr_op_execute``), ordered on ``cfg.stream``."""
+        self._check_open()
+        _check_size(x, int(lib.mr_x_size(ctypes.byref(self._cfg))), "x")
+        if out is not None:
+            _check_size(out, _size(x), "out")
+        else:
+            out = _empty(tuple(x.shape) if _is_torch(x) else x.__cuda_array_interface__["shape"],
+                         "complex64", _device_of(x))
+        check(lib.mr_op_execute(self._handle, _ptr(x, "x", "complex64"),
+                                _ptr(out, "out", "complex64")), "mr_op_execute")
+        return out
+
+    __call__ = apply
+
+    def set_kernel_format(self, fmt: str, keep_complex64: bool = True) -> None:
+        """Store the kernel as ``'complex64'``, ``'bf16'`` or ``'int16'`` (+ scale)."""
+        self._check_open()
+        if fmt not in KERNEL_FORMATS:
+            raise ValueError(f"kernel format must be one of {sorted(KERNEL_FORMATS)}")
+        check(lib.mr_b200_op_set_kernel_format(self._handle, KERNEL_FORMATS[fmt],
+                                               1 if keep_complex64 else 0),
+              "mr_b200_op_set_kernel_format")
+
+    @property
+    def kernel_format(self) -> str:
+        self._check_open()
+        f = ctypes.c_int(0)
+        check(lib.mr_b200_op_kernel_format(self._handle, ctypes.byref(f)),
+              "mr_b200_op_kernel_format")
+        return {v: k for k, v in KERNEL_FORMATS.items()}[f.value]
+
+    @property
+    def launches_per_apply(self) -> int:
+        self._check_open()
+        n = ctypes.c_int(0)
+        check(lib.mr_b200_op_launches(self._handle, ctypes.byref(n)), "mr_b200_op_launches")
+        return int(n.value)
+
+    @property
+    def info(self) -> dict:
+        self._check_open()
+        inf = MROpInfo()
+        check(lib.mr_op_info(self._handle, ctypes.byref(inf)), "mr_op_info")
+        n = inf.n_devices
+        return dict(
+            method=OpMethod._TO_STR.get(int(inf.method), "unknown"),
+            devices=list(inf.devices[:n]), coil_begin=list(inf.coil_begin[:n]),
+            coil_count=list(inf.coil_count[:n]), group=list(inf.group[:n]),
+            n_split_coils=int(inf.n_split_coils), peer_access=bool(inf.peer_access),
+            peer_bandwidth_gbs=float(inf.peer_bandwidth_gbs),
+            toep_source=OP_TOEP_SOURCES.get(int(inf.toep_source), "unknown"),
+            toep_devices=int(inf.toep_devices), toep_ms=float(inf.toep_ms),
+            toep_component_ms=float(inf.toep_component_ms),
+            toep_gather_gbs=float(inf.toep_gather_gbs), create_ms=float(inf.create_ms),
+        )
+
+    def kernel(self, k: int = 0):
+        """Read-only view of the operator's complex64 kernel (``mr_op_kernel``)."""
+        self._check_open()
+        ptr = ctypes.c_void_p()
+        check(lib.mr_op_kernel(self._handle, int(k), ctypes.byref(ptr)), "mr_op_kernel")
+        shape = phi2_toep_shape(self._cfg)
+        size = int(lib.mr_phi2_toep_size(ctypes.byref(self._cfg)))
+        torch = _torch()
+
+        class _View:
+            def __init__(self, p, n, owner):
+                self.__cuda_array_interface__ = {
+                    "shape": (n,), "typestr": "<c8", "data": (p, True), "version": 3,
+                    "strides": None}
+                self._owner = owner
+
+        view = torch.as_tensor(_View(ptr.value, size, self), device=self._device)
+        return view.view(shape)
+
+    def close(self) -> None:
+        if self._handle:
+            lib.mr_op_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+        self._keep = ()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass
+
+
+def create_op(cfg: MRConfig, SEs, phi2, traj, mask=None, **kwargs) -> AhAOp:
+    """Alias of :meth:`AhAOp.create_op` (reference ``api.py:1237-1255``)."""
+    return AhAOp.create_op(cfg, SEs, phi2, traj, mask, **kwargs)

@@ -1,0 +1,575 @@
+// Stateless apply plan: mr_aha_plan_create / execute / destroy and the
+// one-shot mr_aha_toeplitz (reference src/cuda/mr_aha.cu:375-834).
+//
+// Data flow of one execute, per coil group of G coils (P = G * L planes,
+// plane p = c * L + l), for an image [Nx, Ny, Nz] and grid [Mx, My, Mz]:
+//
+//   pass 1 (3D / stack): z lines. Reads x and SEs, forms S_c x_l, transforms
+//          along z (zero-padded to Mz) -> W0 [P][Mz][Ny][Nx].
+//   pass 2: y lines. Reads W0 (or, in 2D, x * SEs directly), transforms
+//          along y (zero-padded to My) -> W1 [P][Mz][My][Nx].
+//   pass 3: x lines. Reads W1 rows, transforms along x (zero-padded to Mx),
+//          multiplies every frequency's rank vector of every coil by the
+//          packed Hermitian block, transforms back and crops to Nx -> W1
+//          (in place).
+//   pass 4: y lines back, cropped to Ny -> W0 (2D: conj(S_c) coil sum into
+//          the output).
+//   pass 5 (3D / stack): z lines back, cropped to Nz, multiplied by
+//          conj(S_c) and summed over the group's coils into the output.
+//
+// The full upsampled spectrum is never written to memory: x is the last
+// forward and first inverse axis, so only half-padded intermediates
+// (Mz*My*Nx and Mz*Ny*Nx per plane) go through HBM. When the L lines of one
+// coil do not fit in shared memory, pass 3 falls back to a plain x transform
+// into a full-grid buffer, a stand-alone block multiply and a plain inverse.
+#include "engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+struct mr_aha_plan_s {
+    mr_config cfg;
+    mr_geom g;
+    cudaStream_t stream;
+    int group;       // coils per group
+    mr_fft_axis ax[3];
+    float2 *d_tw;    // twiddle tables of the three axes
+    float2 *W0, *W1; // intermediates
+    float2 *W2, *W3; // unfused pass 3 only: full-grid spectrum in / out
+    int *d_inv;      // masked: natural grid index -> mask row
+    int fused;       // pass 3 with the block multiply inside
+    int nc_cta;      // coils per CTA in the fused pass 3
+    int xt_z, xt_y;  // strided tile widths
+    int launches;    // kernels per execute (accounting)
+};
+
+// ---------------------------------------------------------------------------
+// Stand-alone block multiply over a full-grid buffer (unfused pass 3)
+// ---------------------------------------------------------------------------
+
+template <int KF>
+__global__ void __launch_bounds__(256) k_bd_full(const float2 *__restrict__ in,
+                                                 float2 *__restrict__ out, mr_geom g,
+                                                 mr_kernel_ref K, int ncoil) {
+    const int64_t vpad = g.vpad;
+    const int64_t total = vpad * ncoil * g.L;
+    for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < total;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t q = w % vpad;
+        const int64_t rest = w / vpad;
+        const int c = (int)(rest % g.L);
+        const int k = (int)(rest / g.L);
+        const int jx = (int)(q % g.m[0]);
+        const int jy = (int)((q / g.m[0]) % g.m[1]);
+        const int jz = (int)(q / ((int64_t)g.m[0] * g.m[1]));
+        int64_t row;
+        bool zero = false;
+        if (K.inv) {
+            const int r = __ldg(K.inv + q);
+            zero = r < 0;
+            row = zero ? 0 : r;
+        } else {
+            row = mr_nat2cent_d(jx, g.m[0], g.cm[0]) +
+                  (int64_t)g.m[0] * (mr_nat2cent_d(jy, g.m[1], g.cm[1]) +
+                                     (int64_t)g.m[1] * mr_nat2cent_d(jz, g.m[2], g.cm[2]));
+        }
+        float2 y = make_float2(0.f, 0.f);
+        if (!zero) {
+            const mr_kload<KF> kl = mr_kload_at<KF>(K, row);
+            y = bd_one<KF>(in + (int64_t)k * g.L * vpad + q, vpad, g.L, c, kl, g.upper);
+        }
+        out[w] = y;
+    }
+}
+
+static int launch_bd_full(const float2 *in, float2 *out, const mr_geom &g,
+                          const mr_kernel_ref &K, int ncoil, cudaStream_t s) {
+    const int64_t total = g.vpad * ncoil * g.L;
+    const int64_t blocks = std::min<int64_t>(mr_cdiv(total, 256), 148 * 64);
+    switch (K.kf) {
+        case MR_KF_F32: k_bd_full<MR_KF_F32><<<(unsigned)blocks, 256, 0, s>>>(in, out, g, K, ncoil); break;
+        case MR_KF_BF16: k_bd_full<MR_KF_BF16><<<(unsigned)blocks, 256, 0, s>>>(in, out, g, K, ncoil); break;
+        case MR_KF_I16: k_bd_full<MR_KF_I16><<<(unsigned)blocks, 256, 0, s>>>(in, out, g, K, ncoil); break;
+        default: MR_FAIL(MR_ERR_INTERNAL, "unknown kernel format");
+    }
+    MR_LAUNCH_CHECK("k_bd_full");
+    return MR_SUCCESS;
+}
+
+// Grid -> mask row map (reference mr_kernels.cu:259-278): entries outside
+// the mask stay -1 from the preceding memset.
+__global__ void k_mask_inverse(int *inv, const int64_t *__restrict__ mask, int64_t nm,
+                               mr_geom g) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nm) return;
+    int64_t c = mask[i];
+    const int kx = (int)(c % g.m[0]);
+    c /= g.m[0];
+    const int ky = (int)(c % g.m[1]);
+    const int kz = (int)(c / g.m[1]);
+    auto c2n = [](int k, int M, int cm) {
+        const int j = k - cm;
+        return j < 0 ? j + M : j;
+    };
+    const int64_t nat = c2n(kx, g.m[0], g.cm[0]) +
+                        (int64_t)g.m[0] * (c2n(ky, g.m[1], g.cm[1]) +
+                                           (int64_t)g.m[1] * c2n(kz, g.m[2], g.cm[2]));
+    inv[nat] = (int)i;
+}
+
+// ---------------------------------------------------------------------------
+// Plan construction
+// ---------------------------------------------------------------------------
+
+static void plan_release(mr_aha_plan p) {
+    if (p->d_tw) cudaFree(p->d_tw);
+    if (p->W0) cudaFree(p->W0);
+    if (p->W1) cudaFree(p->W1);
+    if (p->W2) cudaFree(p->W2);
+    if (p->W3) cudaFree(p->W3);
+    if (p->d_inv) cudaFree(p->d_inv);
+    p->d_tw = nullptr;
+    p->W0 = p->W1 = p->W2 = p->W3 = nullptr;
+    p->d_inv = nullptr;
+    cudaGetLastError();
+}
+
+static size_t plan_bytes(const mr_aha_plan p, int group) {
+    const mr_geom &g = p->g;
+    const size_t P = (size_t)group * g.L;
+    const bool has_z = p->cfg.n_spatial == 3;
+    size_t b = P * g.m[2] * g.m[1] * g.n[0];                // W1
+    if (has_z) b += P * g.m[2] * g.n[1] * g.n[0];           // W0
+    if (!p->fused) b += 2 * P * (size_t)g.vpad;             // W2, W3
+    b *= sizeof(float2);
+    if (p->cfg.is_masked) b += (size_t)g.vpad * sizeof(int);
+    return b;
+}
+
+static int plan_alloc(mr_aha_plan p, int group) {
+    const mr_geom &g = p->g;
+    const size_t P = (size_t)group * g.L;
+    const bool has_z = p->cfg.n_spatial == 3;
+    cudaError_t e = cudaSuccess;
+    if (has_z) e = cudaMalloc(&p->W0, P * g.m[2] * g.n[1] * g.n[0] * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMalloc(&p->W1, P * g.m[2] * g.m[1] * g.n[0] * sizeof(float2));
+    if (e == cudaSuccess && !p->fused) e = cudaMalloc(&p->W2, P * g.vpad * sizeof(float2));
+    if (e == cudaSuccess && !p->fused) e = cudaMalloc(&p->W3, P * g.vpad * sizeof(float2));
+    if (e == cudaSuccess && p->cfg.is_masked) e = cudaMalloc(&p->d_inv, g.vpad * sizeof(int));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        if (p->W0) cudaFree(p->W0);
+        if (p->W1) cudaFree(p->W1);
+        if (p->W2) cudaFree(p->W2);
+        if (p->W3) cudaFree(p->W3);
+        if (p->d_inv) cudaFree(p->d_inv);
+        p->W0 = p->W1 = p->W2 = p->W3 = nullptr;
+        p->d_inv = nullptr;
+        MR_FAIL(MR_ERR_ALLOC, "failed to allocate the work buffers for a group of %d coil(s): %s",
+                group, cudaGetErrorString(e));
+    }
+    p->group = group;
+    return MR_SUCCESS;
+}
+
+static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
+    int rc = mr_config_validate(cfg);
+    if (rc != MR_SUCCESS) return rc;
+    mr_aha_plan p = (mr_aha_plan)calloc(1, sizeof(struct mr_aha_plan_s));
+    if (!p) MR_FAIL(MR_ERR_ALLOC, "failed to allocate the plan struct");
+    p->cfg = *cfg;
+    p->stream = (cudaStream_t)cfg->stream;
+    mr_geom_from_config(cfg, &p->g);
+    const mr_geom &g = p->g;
+
+    // FFT factorisations and twiddle tables of the three axes.
+    int off[3], tot = 0;
+    for (int d = 0; d < 3; ++d) {
+        rc = mr_fft_factor(g.m[d], &p->ax[d]);
+        if (rc != MR_SUCCESS) {
+            free(p);
+            return rc;
+        }
+        off[d] = tot;
+        tot += g.m[d];
+    }
+    std::vector<float2> h(tot);
+    for (int d = 0; d < 3; ++d) mr_fft_twiddles(g.m[d], h.data() + off[d]);
+    if (cudaMalloc(&p->d_tw, tot * sizeof(float2)) != cudaSuccess) {
+        cudaGetLastError();
+        free(p);
+        MR_FAIL(MR_ERR_ALLOC, "failed to allocate the FFT tables");
+    }
+    if (cudaMemcpy(p->d_tw, h.data(), tot * sizeof(float2), cudaMemcpyHostToDevice) !=
+        cudaSuccess) {
+        plan_release(p);
+        free(p);
+        MR_FAIL(MR_ERR_CUDA, "failed to upload the FFT tables");
+    }
+    for (int d = 0; d < 3; ++d) p->ax[d].tw = p->d_tw + off[d];
+
+    // Pass geometry: strided tile widths and the fused pass 3.
+    const size_t lim = (size_t)mr_smem_limit();
+    const size_t half = lim / 2;  // aim for two CTAs per SM on strided passes
+    p->xt_z = mr_pick_xt(g.m[2], g.m[2], MR_SM_COILSUM, g.n[0], half);
+    p->xt_y = mr_pick_xt(g.m[1], g.m[1], MR_SM_COILSUM, g.n[0], half);
+    if (mr_strided_smem(g.m[2], p->xt_z, g.m[2], MR_SM_COILSUM) > lim ||
+        mr_strided_smem(g.m[1], p->xt_y, g.m[1], MR_SM_COILSUM) > lim) {
+        plan_release(p);
+        free(p);
+        MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d / %d points exceeds shared memory",
+                g.m[1], g.m[2]);
+    }
+    p->nc_cta = 1;
+    p->fused = mr_xbd_smem(g.m[0], g.L, 1) <= lim;
+    if (p->fused && g.L <= 16 && mr_xbd_smem(g.m[0], g.L, 2) <= lim && cfg->n_coils >= 2)
+        p->nc_cta = 2;
+    if (!p->fused && mr_xplain_smem(g.m[0], 1) > lim) {
+        plan_release(p);
+        free(p);
+        MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d points exceeds shared memory", g.m[0]);
+    }
+    if (mr_env_int("MR_AHA_B200_UNFUSED_BD", 0)) p->fused = 0;
+
+    // Coil group: all coils if they fit the budget, else fewer.
+    size_t budget = 0;
+    rc = mr_memory_budget(cfg, &budget);
+    if (rc != MR_SUCCESS) {
+        plan_release(p);
+        free(p);
+        return rc;
+    }
+    int group = mr_env_int("MR_AHA_CUDA_COIL_GROUP", cfg->n_coils);
+    if (group < 1 || group > cfg->n_coils) group = cfg->n_coils;
+    while (group > 1 && plan_bytes(p, group) > budget) --group;
+    for (;; --group) {
+        rc = plan_alloc(p, group);
+        if (rc == MR_SUCCESS || group == 1) break;
+    }
+    if (rc != MR_SUCCESS) {
+        plan_release(p);
+        free(p);
+        return rc;
+    }
+    mr_clear_error();
+    const int ngroups = (int)mr_cdiv(cfg->n_coils, group);
+    const int per = (cfg->n_spatial == 3 ? 2 : 0) + 2 + (p->fused ? 1 : 3);
+    p->launches = ngroups * per + (cfg->is_masked ? 1 : 0);
+    if (cfg->verbose)
+        printf("[mr_aha] plan: %s block multiply, %d coil(s) per group, tiles z %d y %d\n",
+               p->fused ? "fused" : "stand-alone", p->group, p->xt_z, p->xt_y);
+    *out = p;
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_aha_plan_create(const mr_config *cfg, mr_aha_plan *plan_out) {
+    mr_clear_error();
+    MR_REQUIRE(plan_out != nullptr, "mr_aha_plan_create: plan_out is NULL");
+    *plan_out = nullptr;
+    MR_REQUIRE(cfg != nullptr, "mr_aha_plan_create: cfg is NULL");
+    int prev = -1;
+    int rc = mr_push_device(cfg, &prev);
+    if (rc == MR_SUCCESS) rc = plan_create_impl(cfg, plan_out);
+    mr_pop_device(prev);
+    return rc;
+}
+
+extern "C" int mr_aha_plan_destroy(mr_aha_plan plan) {
+    mr_clear_error();
+    if (!plan) return MR_SUCCESS;
+    int prev = -1;
+    (void)mr_push_device(&plan->cfg, &prev);
+    plan_release(plan);
+    mr_pop_device(prev);
+    free(plan);
+    return MR_SUCCESS;
+}
+
+int mr_plan_group(mr_aha_plan plan) { return plan->group; }
+cudaStream_t mr_plan_stream(mr_aha_plan plan) { return plan->stream; }
+int mr_plan_launch_count(mr_aha_plan plan) { return plan->launches; }
+
+// ---------------------------------------------------------------------------
+// Execution
+// ---------------------------------------------------------------------------
+
+int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
+                      const mr_kernel_ref &K0, const int64_t *d_mask, float2 *out,
+                      cudaStream_t s) {
+    const mr_config &cfg = p->cfg;
+    const mr_geom &g = p->g;
+    const bool has_z = cfg.n_spatial == 3;
+    const int Nx = g.n[0], Ny = g.n[1], Nz = g.n[2];
+    const int Mx = g.m[0], My = g.m[1], Mz = g.m[2];
+    mr_kernel_ref K = K0;
+    int rc;
+
+    if (cfg.is_masked) {
+        const int64_t nm = cfg.num_masked;
+        MR_CUDA_TRY(cudaMemsetAsync(p->d_inv, 0xFF, g.vpad * sizeof(int), s));
+        k_mask_inverse<<<(unsigned)mr_cdiv(nm, 256), 256, 0, s>>>(p->d_inv, d_mask, nm, g);
+        MR_LAUNCH_CHECK("k_mask_inverse");
+        K.inv = p->d_inv;
+        K.stride = nm;
+    } else {
+        K.inv = nullptr;
+        K.stride = g.vpad;
+    }
+
+    for (int c0 = 0; c0 < cfg.n_coils; c0 += p->group) {
+        const int G = std::min(p->group, cfg.n_coils - c0);
+        const int P = G * g.L;
+        const int accumulate = c0 > 0;
+        const int64_t w0_plane = (int64_t)Mz * Ny * Nx;
+        const int64_t w1_plane = (int64_t)Mz * My * Nx;
+
+        // ---- pass 1: z lines, S_c x_l, zero-pad along z ----
+        if (has_z) {
+            mr_strided_args a;
+            std::memset(&a, 0, sizeof(a));
+            a.ax = p->ax[2];
+            a.nfast = Nx;
+            a.xt = p->xt_z;
+            a.nxt = (int)mr_cdiv(Nx, a.xt);
+            a.nouter = Ny;
+            a.nplane = P;
+            a.s_outer = Nx;
+            a.s_axis = (int64_t)Nx * Ny;
+            a.n_in = Nz;
+            a.shift_in = g.cn[2];
+            a.xs_x = x;
+            a.xs_s = S;
+            a.img_plane = g.vimg;
+            a.L = g.L;
+            a.coil0 = c0;
+            a.dst = p->W0;
+            a.d_plane = w0_plane;
+            a.d_outer = Nx;
+            a.d_axis = (int64_t)Ny * Nx;
+            a.n_out = Mz;
+            a.shift_out = 0;
+            a.scale = 1.f;
+            rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
+            if (rc != MR_SUCCESS) return rc;
+        }
+        // ---- pass 2: y lines, zero-pad along y ----
+        {
+            mr_strided_args a;
+            std::memset(&a, 0, sizeof(a));
+            a.ax = p->ax[1];
+            a.nfast = Nx;
+            a.xt = p->xt_y;
+            a.nxt = (int)mr_cdiv(Nx, a.xt);
+            a.nouter = Mz;
+            a.nplane = P;
+            a.n_in = Ny;
+            a.shift_in = g.cn[1];
+            a.L = g.L;
+            a.coil0 = c0;
+            a.img_plane = g.vimg;
+            a.dst = p->W1;
+            a.d_plane = w1_plane;
+            a.d_outer = (int64_t)My * Nx;
+            a.d_axis = Nx;
+            a.n_out = My;
+            a.shift_out = 0;
+            a.scale = 1.f;
+            if (has_z) {
+                a.src = p->W0;
+                a.s_plane = w0_plane;
+                a.s_outer = (int64_t)Ny * Nx;
+                a.s_axis = Nx;
+                rc = mr_launch_strided(-1, MR_LM_BUF, MR_SM_BUF, a, s);
+            } else {
+                a.xs_x = x;
+                a.xs_s = S;
+                a.s_outer = 0;
+                a.s_axis = Nx;
+                rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
+            }
+            if (rc != MR_SUCCESS) return rc;
+        }
+        // ---- pass 3: x lines with the block multiply ----
+        {
+            mr_x_args a;
+            std::memset(&a, 0, sizeof(a));
+            a.ax = p->ax[0];
+            a.scale = 1.f;
+            if (p->fused) {
+                a.src = p->W1;
+                a.dst = p->W1;
+                a.s_row = Nx;
+                a.d_row = Nx;
+                a.n_in = Nx;
+                a.shift_in = g.cn[0];
+                a.n_out = Nx;
+                a.shift_out = g.cn[0];
+                a.plane_rows = (int64_t)My * Mz;
+                a.nloc = My * Mz;
+                a.nc = p->nc_cta;
+                a.ncoil = G;
+                a.nchunk = (int)mr_cdiv(G, a.nc);
+                a.L = g.L;
+                a.upper = g.upper;
+                a.My = My;
+                a.Mz = Mz;
+                a.cmx = g.cm[0];
+                a.cmy = g.cm[1];
+                a.cmz = g.cm[2];
+                a.K = K;
+                rc = mr_launch_xbd(a, s);
+                if (rc != MR_SUCCESS) return rc;
+            } else {
+                const int rows = 4;
+                a.rows_cta = rows;
+                a.src = p->W1;
+                a.dst = p->W2;
+                a.s_row = Nx;
+                a.d_row = Mx;
+                a.nrows = (int64_t)P * My * Mz;
+                a.n_in = Nx;
+                a.shift_in = g.cn[0];
+                a.n_out = Mx;
+                a.shift_out = 0;
+                rc = mr_launch_xplain(-1, a, s);
+                if (rc != MR_SUCCESS) return rc;
+                rc = launch_bd_full(p->W2, p->W3, g, K, G, s);
+                if (rc != MR_SUCCESS) return rc;
+                a.src = p->W3;
+                a.dst = p->W1;
+                a.s_row = Mx;
+                a.d_row = Nx;
+                a.n_in = Mx;
+                a.shift_in = 0;
+                a.n_out = Nx;
+                a.shift_out = g.cn[0];
+                rc = mr_launch_xplain(1, a, s);
+                if (rc != MR_SUCCESS) return rc;
+            }
+        }
+        // ---- pass 4: y lines back, crop ----
+        {
+            mr_strided_args a;
+            std::memset(&a, 0, sizeof(a));
+            a.ax = p->ax[1];
+            a.nfast = Nx;
+            a.xt = p->xt_y;
+            a.nxt = (int)mr_cdiv(Nx, a.xt);
+            a.nouter = Mz;
+            a.src = p->W1;
+            a.s_plane = w1_plane;
+            a.s_outer = (int64_t)My * Nx;
+            a.s_axis = Nx;
+            a.n_in = My;
+            a.shift_in = 0;
+            a.n_out = Ny;
+            a.shift_out = g.cn[1];
+            a.L = g.L;
+            a.coil0 = c0;
+            a.img_plane = g.vimg;
+            a.scale = 1.f;
+            if (has_z) {
+                a.nplane = P;
+                a.dst = p->W0;
+                a.d_plane = w0_plane;
+                a.d_outer = (int64_t)Ny * Nx;
+                a.d_axis = Nx;
+                rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_BUF, a, s);
+            } else {
+                a.nplane = g.L;
+                a.xs_s = S;
+                a.dst = out;
+                a.d_plane = g.vimg;
+                a.d_outer = 0;
+                a.d_axis = Nx;
+                a.ncoil = G;
+                a.accumulate = accumulate;
+                rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
+            }
+            if (rc != MR_SUCCESS) return rc;
+        }
+        // ---- pass 5: z lines back, crop, conj(S_c) coil sum ----
+        if (has_z) {
+            mr_strided_args a;
+            std::memset(&a, 0, sizeof(a));
+            a.ax = p->ax[2];
+            a.nfast = Nx;
+            a.xt = p->xt_z;
+            a.nxt = (int)mr_cdiv(Nx, a.xt);
+            a.nouter = Ny;
+            a.nplane = g.L;
+            a.src = p->W0;
+            a.s_plane = w0_plane;
+            a.s_outer = Nx;
+            a.s_axis = (int64_t)Ny * Nx;
+            a.n_in = Mz;
+            a.shift_in = 0;
+            a.n_out = Nz;
+            a.shift_out = g.cn[2];
+            a.L = g.L;
+            a.coil0 = c0;
+            a.xs_s = S;
+            a.img_plane = g.vimg;
+            a.dst = out;
+            a.d_plane = g.vimg;
+            a.d_outer = Nx;
+            a.d_axis = (int64_t)Ny * Nx;
+            a.ncoil = G;
+            a.accumulate = accumulate;
+            a.scale = 1.f;
+            rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
+            if (rc != MR_SUCCESS) return rc;
+        }
+    }
+    if (cfg.verbose) {
+        MR_CUDA_TRY(cudaStreamSynchronize(s));
+        printf("[mr_aha] AhA applied over %d coil(s) in groups of %d, grid [%d %d %d] -> "
+               "[%d %d %d], L = %d%s\n",
+               cfg.n_coils, p->group, Nx, Ny, Nz, Mx, My, Mz, g.L,
+               cfg.is_masked ? ", masked" : "");
+    }
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_aha_plan_execute(mr_aha_plan plan, const mr_complex *d_x,
+                                   const mr_complex *d_SEs,
+                                   const mr_complex *d_phi2_toep, const int64_t *d_mask,
+                                   mr_complex *d_AhAx) {
+    mr_clear_error();
+    MR_REQUIRE(plan != nullptr, "mr_aha_plan_execute: plan is NULL");
+    MR_REQUIRE(d_x != nullptr, "mr_aha_plan_execute: d_x is NULL");
+    MR_REQUIRE(d_SEs != nullptr, "mr_aha_plan_execute: d_SEs is NULL");
+    MR_REQUIRE(d_phi2_toep != nullptr, "mr_aha_plan_execute: d_phi2_toep is NULL");
+    MR_REQUIRE(d_AhAx != nullptr, "mr_aha_plan_execute: d_AhAx is NULL");
+    MR_REQUIRE((const void *)d_AhAx != (const void *)d_x,
+               "mr_aha_plan_execute: d_AhAx must not alias d_x");
+    if (plan->cfg.is_masked)
+        MR_REQUIRE(d_mask != nullptr,
+                   "mr_aha_plan_execute: d_mask is required when is_masked is set");
+    mr_kernel_ref K;
+    std::memset(&K, 0, sizeof(K));
+    K.data = d_phi2_toep;
+    K.kf = MR_KF_F32;
+    int prev = -1;
+    int rc = mr_push_device(&plan->cfg, &prev);
+    if (rc == MR_SUCCESS)
+        rc = mr_plan_execute_k(plan, reinterpret_cast<const float2 *>(d_x),
+                               reinterpret_cast<const float2 *>(d_SEs), K, d_mask,
+                               reinterpret_cast<float2 *>(d_AhAx), plan->stream);
+    mr_pop_device(prev);
+    return rc;
+}
+
+extern "C" int mr_aha_toeplitz(const mr_config *cfg, const mr_complex *d_x,
+                               const mr_complex *d_SEs, const mr_complex *d_phi2_toep,
+                               const int64_t *d_mask, mr_complex *d_AhAx) {
+    mr_aha_plan plan = nullptr;
+    int rc = mr_aha_plan_create(cfg, &plan);
+    if (rc != MR_SUCCESS) return rc;
+    rc = mr_aha_plan_execute(plan, d_x, d_SEs, d_phi2_toep, d_mask, d_AhAx);
+    // Work is asynchronous: make sure it finished before the buffers go.
+    cudaStreamSynchronize(plan->stream);
+    const int rc2 = mr_aha_plan_destroy(plan);
+    return rc != MR_SUCCESS ? rc : rc2;
+}

@@ -1,0 +1,144 @@
+// Device code of the block-diagonal Toeplitz multiply: at every upsampled
+// k-space location the rank row vector of each coil is multiplied from the
+// right by the location's Hermitian L x L block, y_c = sum_r v_r A_rc
+// (reference include/mr_aha/mr_aha.h:48-62, src/cuda/mr_kernels_bd.cu:56-139).
+// The block is stored as one packed triangle; each stored element A_rc is
+// read once and contributes A_rc v_r to y_c and, off the diagonal,
+// conj(A_rc) v_c to y_r.
+//
+// Kernel storage formats (template parameter KF):
+//   0: complex64 elements, component t of location q at base[q + t * stride];
+//   1: bfloat16 (re, im) pairs with one float scale per location;
+//   2: int16 (re, im) pairs with one float scale per location (block
+//      floating point: value = scale * int16).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft_device.cuh"
+
+#define MR_KF_F32 0
+#define MR_KF_BF16 1
+#define MR_KF_I16 2
+
+struct mr_kernel_ref {
+    const void *data;     // element array (format KF)
+    const float *scale;   // per-location scale (KF 1, 2), indexed like the location
+    int64_t stride;       // elements between consecutive packed components
+    const int *inv;       // masked: natural grid index -> mask row, -1 outside; else NULL
+    int kf;
+};
+
+template <int KF>
+struct mr_kload {
+    const void *base;
+    int64_t stride;
+    float s;
+    __device__ __forceinline__ float2 get(int t) const {
+        if constexpr (KF == MR_KF_F32) {
+            return __ldg(reinterpret_cast<const float2 *>(base) + (int64_t)t * stride);
+        } else if constexpr (KF == MR_KF_BF16) {
+            const __nv_bfloat162 v =
+                __ldg(reinterpret_cast<const __nv_bfloat162 *>(base) + (int64_t)t * stride);
+            const float2 f = __bfloat1622float2(v);
+            return make_float2(f.x * s, f.y * s);
+        } else {
+            const short2 v = __ldg(reinterpret_cast<const short2 *>(base) + (int64_t)t * stride);
+            return make_float2((float)v.x * s, (float)v.y * s);
+        }
+    }
+};
+
+// Loader for the block of location `loc` (row in the kernel array).
+template <int KF>
+__device__ __forceinline__ mr_kload<KF> mr_kload_at(const mr_kernel_ref &k, int64_t loc) {
+    mr_kload<KF> l;
+    if constexpr (KF == MR_KF_F32) {
+        l.base = reinterpret_cast<const float2 *>(k.data) + loc;
+        l.s = 1.0f;
+    } else if constexpr (KF == MR_KF_BF16) {
+        l.base = reinterpret_cast<const __nv_bfloat162 *>(k.data) + loc;
+        l.s = __ldg(k.scale + loc);
+    } else {
+        l.base = reinterpret_cast<const short2 *>(k.data) + loc;
+        l.s = __ldg(k.scale + loc);
+    }
+    l.stride = k.stride;
+    return l;
+}
+
+// y[k] = v[k] A for NC vectors of compile-time rank L, walking the packed
+// triangle once. All register indices are compile-time constants after
+// unrolling.
+template <int L, int NC, int KF>
+__device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[NC][L],
+                                         const mr_kload<KF> &kl, int upper) {
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int i = 0; i < L; ++i) y[k][i] = make_float2(0.f, 0.f);
+    int t = 0;
+    if (!upper) {
+#pragma unroll
+        for (int c = 0; c < L; ++c) {
+#pragma unroll
+            for (int r = c; r < L; ++r) {
+                const float2 a = kl.get(t++);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    y[k][c] = c_add(y[k][c], c_mul(a, v[k][r]));
+                    if (r != c) y[k][r] = c_add(y[k][r], c_mulc(a, v[k][c]));
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < L; ++c) {
+#pragma unroll
+            for (int r = 0; r <= c; ++r) {
+                const float2 a = kl.get(t++);
+#pragma unroll
+                for (int k = 0; k < NC; ++k) {
+                    y[k][c] = c_add(y[k][c], c_mul(a, v[k][r]));
+                    if (r != c) y[k][r] = c_add(y[k][r], c_mulc(a, v[k][c]));
+                }
+            }
+        }
+    }
+}
+
+// Packed offset of element (i, j) of the block and whether the stored value
+// must be conjugated (the element lies in the unstored triangle).
+__device__ __forceinline__ int bd_tri_offset(int i, int j, int L, int upper, bool *cj) {
+    int r = i, c = j;
+    *cj = false;
+    if (upper) {
+        if (r > c) { int t = r; r = c; c = t; *cj = true; }
+        return c * (c + 1) / 2 + r;
+    }
+    if (r < c) { int t = r; r = c; c = t; *cj = true; }
+    return c * L - c * (c - 1) / 2 + (r - c);
+}
+
+// Runtime-rank variant: one output component y_c = sum_r v_r A_rc, with v
+// read from `v` (element r at v[r * vs]).
+template <int KF>
+__device__ __forceinline__ float2 bd_one(const float2 *v, int64_t vs, int L, int c,
+                                         const mr_kload<KF> &kl, int upper) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int r = 0; r < L; ++r) {
+        bool cj;
+        const int t = bd_tri_offset(r, c, L, upper, &cj);
+        float2 a = kl.get(t);
+        if (cj) a = c_conj(a);
+        acc = c_add(acc, c_mul(a, v[(int64_t)r * vs]));
+    }
+    return acc;
+}
+
+__device__ __forceinline__ int mr_nat2cent_d(int j, int M, int c) {
+    int k = j + c;
+    return k >= M ? k - M : k;
+}

@@ -1,0 +1,95 @@
+// Internal interface of the apply engine (plans, passes, FFT tables) shared
+// by the apply entry points, the operator object, the kernel builder and the
+// precision / CG extensions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "bd_device.cuh"
+#include "fft_device.cuh"
+#include "mr_internal.h"
+
+// Factor M into supported radices; returns MR_SUCCESS or MR_ERR_UNSUPPORTED.
+int mr_fft_factor(int M, mr_fft_axis *ax);
+// Fill the twiddle table W_M^e (e < M) into host memory `h` (float2[M]).
+void mr_fft_twiddles(int M, float2 *h);
+
+// Pass descriptions -------------------------------------------------------
+
+// Lines along a strided axis; a CTA transforms `xt` consecutive positions of
+// the contiguous (x) dimension for one (outer, plane).
+#define MR_LM_BUF 0
+#define MR_LM_XS 1
+#define MR_SM_BUF 0
+#define MR_SM_COILSUM 1
+
+struct mr_strided_args {
+    mr_fft_axis ax;
+    int nfast, xt, nxt, nouter, nplane;
+    // source: BUF mode reads src; XS mode reads x (plane l) times S (coil)
+    const float2 *src;
+    int64_t s_plane, s_outer, s_axis;
+    int n_in, shift_in;
+    const float2 *xs_x;
+    const float2 *xs_s;
+    int64_t img_plane;   // elements of one image volume (x plane / S plane)
+    int L, coil0;
+    // destination: BUF mode writes dst; COILSUM writes out (plane l) summing
+    // conj(S_c) * result over ncoil coils
+    float2 *dst;
+    int64_t d_plane, d_outer, d_axis;
+    int n_out, shift_out;
+    int ncoil, accumulate;
+    float scale;
+};
+
+// Lines along the contiguous axis (rows). Plain mode: rows r of src (stride
+// s_row) to rows of dst (stride d_row). Block-diagonal mode: the CTA holds
+// the L lines of nc coils at one (jy, jz) location and multiplies each
+// frequency by the kernel block between the forward and inverse transform.
+struct mr_x_args {
+    mr_fft_axis ax;
+    const float2 *src;
+    float2 *dst;
+    int64_t s_row, d_row;
+    int64_t nrows;
+    int rows_cta;
+    int n_in, shift_in, n_out, shift_out;
+    float scale;
+    // block-diagonal mode
+    int64_t plane_rows;  // rows per plane (My * Mz)
+    int nloc;            // locations (My * Mz)
+    int nchunk;          // coil chunks
+    int nc;              // coils per CTA (last chunk may have fewer)
+    int ncoil;           // coils in the group
+    int L, upper;
+    int My, Mz, cmx, cmy, cmz;
+    mr_kernel_ref K;
+};
+
+int mr_launch_strided(int dir, int lmode, int smode, const mr_strided_args &a,
+                      cudaStream_t s);
+int mr_launch_xplain(int dir, const mr_x_args &a, cudaStream_t s);
+int mr_launch_xbd(const mr_x_args &a, cudaStream_t s);
+
+// Shared-memory bytes of a strided pass with tile width xt.
+size_t mr_strided_smem(int M, int xt, int n_out, int smode);
+// Largest power-of-two tile width (<= cap) that fits `limit` bytes.
+int mr_pick_xt(int M, int n_out, int smode, int nfast, size_t limit);
+size_t mr_xbd_smem(int M, int L, int nc);
+size_t mr_xplain_smem(int M, int rows);
+
+// Current device ordinal (0..63) and its opt-in shared memory per block.
+int mr_current_device();
+int mr_smem_limit();
+
+// Plan helpers for internal callers --------------------------------------
+
+int mr_plan_execute_k(mr_aha_plan plan, const float2 *x, const float2 *S,
+                      const mr_kernel_ref &K, const int64_t *d_mask, float2 *out,
+                      cudaStream_t s);
+int mr_plan_kf_supported(mr_aha_plan plan);
+int mr_plan_group(mr_aha_plan plan);
+cudaStream_t mr_plan_stream(mr_aha_plan plan);
+// Number of kernels one execute launches (for accounting).
+int mr_plan_launch_count(mr_aha_plan plan);

@@ -1,0 +1,419 @@
+// Operator object: mr_op_create / execute / info / kernel / destroy /
+// abandon (reference src/cuda/mr_op.cu, single-device "direct" path
+// :1034-1304, 1348-1352, 1480-1640).
+//
+// One device: the primary (cfg->gpu_device_id, or the current device for
+// -1). A request for further devices is accepted and served by the primary
+// alone; mr_op_info reports one device. The operator owns (or, with
+// MR_OP_SHARE_PRIMARY, borrows) the maps, the mask and the kernel, and an
+// apply plan. Its kernel can be converted to 16-bit storage with a per-
+// location scale (mr_b200_op_set_kernel_format), in which case the applies
+// read the 16-bit copy.
+#include <algorithm>
+#include <chrono>
+#include <new>
+#include <cstring>
+
+#include "engine.h"
+#include "mr_aha/mr_aha_b200.h"
+
+struct mr_op_s {
+    mr_config cfg;
+    mr_op_options opt;
+    int dev;
+    cudaStream_t stream;
+    mr_aha_plan plan;
+    const float2 *S;        // maps (borrowed or owned)
+    const int64_t *mask;    // mask (borrowed or owned)
+    const float2 *K;        // complex64 kernel, reference layout (borrowed or owned)
+    void *S_own, *mask_own, *K_own;
+    // 16-bit kernel copy (MR_B200_KF_BF16 / MR_B200_KF_I16) and its scales
+    int kf;
+    void *K16;
+    float *K16_scale;
+    mr_op_info_t info;
+};
+
+static void op_release(mr_op op, int skip_device) {
+    if (!skip_device) {
+        if (op->plan) mr_aha_plan_destroy(op->plan);
+        if (op->S_own) cudaFree(op->S_own);
+        if (op->mask_own) cudaFree(op->mask_own);
+        if (op->K_own) cudaFree(op->K_own);
+        if (op->K16) cudaFree(op->K16);
+        if (op->K16_scale) cudaFree(op->K16_scale);
+        cudaGetLastError();
+    }
+    delete op;
+}
+
+static int copy_dev(void **dst, const void *src, size_t bytes, cudaStream_t s) {
+    if (cudaMalloc(dst, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *dst = nullptr;
+        MR_FAIL(MR_ERR_ALLOC, "failed to allocate %zu bytes for an operator copy", bytes);
+    }
+    MR_CUDA_TRY(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    return MR_SUCCESS;
+}
+
+static int op_check(const mr_config *cfg, const mr_op_inputs *in, const mr_op_options *o) {
+    int rc = mr_config_validate(cfg);
+    if (rc != MR_SUCCESS) return rc;
+    MR_REQUIRE(o->method == MR_OP_TOEPLITZ || o->method == MR_OP_NUFFT,
+               "mr_op_create: method = %d is neither MR_OP_TOEPLITZ nor MR_OP_NUFFT",
+               (int)o->method);
+    MR_REQUIRE(in->d_SEs != nullptr, "mr_op_create: d_SEs is NULL");
+    const bool need_gram = o->method == MR_OP_NUFFT || in->d_phi2_toep == nullptr;
+    if (need_gram) {
+        MR_REQUIRE(in->d_phi2 != nullptr, "mr_op_create: d_phi2 is NULL");
+        MR_REQUIRE(in->d_traj != nullptr, "mr_op_create: d_traj is NULL");
+        MR_REQUIRE(in->Ntrajs > 0 && in->Nkx > 0,
+                   "mr_op_create: Ntrajs = %lld and Nkx = %lld must be > 0",
+                   (long long)in->Ntrajs, (long long)in->Nkx);
+    }
+    if (o->method == MR_OP_NUFFT) {
+        MR_REQUIRE(!cfg->is_masked,
+                   "mr_op_create: the NUFFT method has no kernel to mask; set is_masked = 0 "
+                   "(or use the Toeplitz method)");
+        MR_REQUIRE(in->d_phi2_toep == nullptr,
+                   "mr_op_create: d_phi2_toep is only used by the Toeplitz method");
+        MR_FAIL(MR_ERR_UNSUPPORTED,
+                "mr_op_create: the NUFFT method is not built in this library; use "
+                "MR_OP_TOEPLITZ");
+    }
+    if (cfg->is_masked)
+        MR_REQUIRE(in->d_mask != nullptr, "mr_op_create: d_mask is required when is_masked is set");
+    return MR_SUCCESS;
+}
+
+static int op_create_impl(const mr_config *cfg, const mr_op_inputs *in, const mr_op_options *o,
+                          mr_op *out) {
+    const auto t_start = std::chrono::steady_clock::now();
+    int rc = op_check(cfg, in, o);
+    if (rc != MR_SUCCESS) return rc;
+    mr_op op = new (std::nothrow) mr_op_s();
+    if (!op) MR_FAIL(MR_ERR_ALLOC, "failed to allocate the operator");
+    op->cfg = *cfg;
+    op->opt = *o;
+    op->stream = (cudaStream_t)cfg->stream;
+    if (cudaGetDevice(&op->dev) != cudaSuccess) {
+        op_release(op, 1);
+        MR_FAIL(MR_ERR_CUDA, "cudaGetDevice failed");
+    }
+    cudaStream_t s = op->stream;
+    // Inputs produced on the caller's stream must be complete.
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        op_release(op, 1);
+        MR_FAIL(MR_ERR_CUDA, "synchronising the caller's stream failed");
+    }
+    const bool share = (o->flags & MR_OP_SHARE_PRIMARY) != 0;
+    const size_t se_bytes = (size_t)mr_se_size(cfg) * sizeof(float2);
+    const size_t k_bytes = (size_t)mr_phi2_toep_size(cfg) * sizeof(float2);
+    if (share) {
+        op->S = reinterpret_cast<const float2 *>(in->d_SEs);
+        op->mask = in->d_mask;
+    } else {
+        rc = copy_dev(&op->S_own, in->d_SEs, se_bytes, s);
+        if (rc == MR_SUCCESS && cfg->is_masked)
+            rc = copy_dev(&op->mask_own, in->d_mask, (size_t)cfg->num_masked * sizeof(int64_t), s);
+        if (rc != MR_SUCCESS) {
+            op_release(op, 0);
+            return rc;
+        }
+        op->S = (const float2 *)op->S_own;
+        op->mask = (const int64_t *)op->mask_own;
+    }
+    double toep_ms = 0.0;
+    if (in->d_phi2_toep) {
+        if (share) {
+            op->K = reinterpret_cast<const float2 *>(in->d_phi2_toep);
+        } else {
+            rc = copy_dev(&op->K_own, in->d_phi2_toep, k_bytes, s);
+            if (rc != MR_SUCCESS) {
+                op_release(op, 0);
+                return rc;
+            }
+            op->K = (const float2 *)op->K_own;
+        }
+        op->info.toep_source = MR_OP_TOEP_SUPPLIED;
+        op->info.toep_devices = 0;
+    } else {
+        if (cudaMalloc(&op->K_own, k_bytes) != cudaSuccess) {
+            cudaGetLastError();
+            op_release(op, 0);
+            MR_FAIL(MR_ERR_ALLOC, "failed to allocate the %zu-byte Toeplitz kernel", k_bytes);
+        }
+        const auto t0 = std::chrono::steady_clock::now();
+        mr_config c = *cfg;
+        c.gpu_device_id = -1;
+        rc = mr_calc_toep(&c, in->d_phi2, in->d_traj, in->Ntrajs, in->Nkx, op->mask,
+                          (mr_complex *)op->K_own);
+        if (rc != MR_SUCCESS) {
+            char msg[512];
+            snprintf(msg, sizeof(msg), "%s", mr_last_error());
+            op_release(op, 0);
+            mr_set_error("%s", msg);
+            return rc;
+        }
+        toep_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                      .count();
+        op->K = (const float2 *)op->K_own;
+        op->info.toep_source = MR_OP_TOEP_BROADCAST;
+        op->info.toep_devices = 1;
+    }
+    mr_config c = *cfg;
+    c.gpu_device_id = -1;
+    rc = mr_aha_plan_create(&c, &op->plan);
+    if (rc != MR_SUCCESS) {
+        char msg[512];
+        snprintf(msg, sizeof(msg), "%s", mr_last_error());
+        op_release(op, 0);
+        mr_set_error("%s", msg);
+        return rc;
+    }
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        op_release(op, 0);
+        MR_FAIL(MR_ERR_CUDA, "operator creation failed: %s",
+                cudaGetErrorString(cudaGetLastError()));
+    }
+    op->kf = MR_KF_F32;
+    mr_op_info_t &inf = op->info;
+    inf.method = MR_OP_TOEPLITZ;
+    inf.n_devices = 1;
+    inf.devices[0] = op->dev;
+    inf.coil_begin[0] = 0;
+    inf.coil_count[0] = cfg->n_coils;
+    inf.group[0] = mr_plan_group(op->plan);
+    inf.toep_ms = toep_ms;
+    inf.create_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start)
+            .count();
+    *out = op;
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_op_options_defaults(mr_op_options *opt) {
+    mr_clear_error();
+    MR_REQUIRE(opt != nullptr, "mr_op_options_defaults: opt is NULL");
+    std::memset(opt, 0, sizeof(*opt));
+    opt->method = MR_OP_TOEPLITZ;
+    opt->toep_dist = MR_TOEP_DIST_AUTO;
+    opt->flags = MR_OP_SHARE_PRIMARY;
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_op_create(const mr_config *cfg, const mr_op_inputs *in,
+                            const mr_op_options *opt, mr_op *op_out) {
+    mr_clear_error();
+    MR_REQUIRE(op_out != nullptr, "mr_op_create: op_out is NULL");
+    *op_out = nullptr;
+    MR_REQUIRE(cfg != nullptr, "mr_op_create: cfg is NULL");
+    MR_REQUIRE(in != nullptr, "mr_op_create: in is NULL");
+    mr_op_options o;
+    if (opt) o = *opt;
+    else mr_op_options_defaults(&o);
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    int rc = MR_SUCCESS;
+    if (cfg->gpu_device_id >= 0 && cfg->gpu_device_id != prev) {
+        if (cudaSetDevice(cfg->gpu_device_id) != cudaSuccess) {
+            cudaGetLastError();
+            MR_FAIL(MR_ERR_CUDA, "cannot select device %d", cfg->gpu_device_id);
+        }
+    }
+    rc = op_create_impl(cfg, in, &o, op_out);
+    cudaSetDevice(prev);
+    return rc;
+}
+
+static mr_kernel_ref op_kernel_ref(mr_op op) {
+    mr_kernel_ref K;
+    std::memset(&K, 0, sizeof(K));
+    if (op->kf == MR_KF_F32) {
+        K.data = op->K;
+    } else {
+        K.data = op->K16;
+        K.scale = op->K16_scale;
+    }
+    K.kf = op->kf;
+    return K;
+}
+
+int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s) {
+    return mr_plan_execute_k(op->plan, x, op->S, op_kernel_ref(op), op->mask, out, s);
+}
+
+extern "C" int mr_op_execute(mr_op op, const mr_complex *d_x, mr_complex *d_AhAx) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_op_execute: op is NULL");
+    MR_REQUIRE(d_x != nullptr, "mr_op_execute: d_x is NULL");
+    MR_REQUIRE(d_AhAx != nullptr, "mr_op_execute: d_AhAx is NULL");
+    MR_REQUIRE((const void *)d_AhAx != (const void *)d_x,
+               "mr_op_execute: d_AhAx must not alias d_x");
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
+    const int rc = mr_op_execute_on(op, reinterpret_cast<const float2 *>(d_x),
+                                    reinterpret_cast<float2 *>(d_AhAx), op->stream);
+    if (prev != op->dev) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int mr_op_info(mr_op op, mr_op_info_t *info) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_op_info: op is NULL");
+    MR_REQUIRE(info != nullptr, "mr_op_info: info is NULL");
+    *info = op->info;
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_op_kernel(mr_op op, int k, const mr_complex **d_phi2_toep) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_op_kernel: op is NULL");
+    MR_REQUIRE(d_phi2_toep != nullptr, "mr_op_kernel: d_phi2_toep is NULL");
+    if (op->opt.method != MR_OP_TOEPLITZ)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "mr_op_kernel: a NUFFT operator has no kernel");
+    MR_REQUIRE(k >= 0 && k < op->info.n_devices, "mr_op_kernel: device index %d outside [0, %d)",
+               k, op->info.n_devices);
+    if (!op->K)
+        MR_FAIL(MR_ERR_UNSUPPORTED,
+                "mr_op_kernel: the complex64 kernel was released after conversion to 16-bit "
+                "storage");
+    *d_phi2_toep = reinterpret_cast<const mr_complex *>(op->K);
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_op_destroy(mr_op op) {
+    mr_clear_error();
+    if (!op) return MR_SUCCESS;
+    int prev = 0;
+    const cudaError_t ce = cudaGetDevice(&prev);
+    cudaSetDevice(op->dev);
+    cudaStreamSynchronize(op->stream);
+    cudaGetLastError();
+    op_release(op, 0);
+    if (ce == cudaSuccess) cudaSetDevice(prev);
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_op_abandon(mr_op op) {
+    mr_clear_error();
+    if (!op) return MR_SUCCESS;
+    // The primary device was reset: its buffers are gone with the context.
+    if (op->plan) {
+        // the plan's host struct only
+        free(op->plan);
+        op->plan = nullptr;
+    }
+    op_release(op, 1);
+    return MR_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// 16-bit kernel storage
+// ---------------------------------------------------------------------------
+
+// One block per location q: scale_q = max |re|, |im| over its ntri elements
+// divided by the largest code (int16: 32767; bf16: 1, the scale only
+// normalises), then every element is stored relative to it.
+template <int KF>
+__global__ void k_quantize(void *out, float *scale, const float2 *__restrict__ K, int64_t nloc,
+                           int64_t ntri) {
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nloc;
+         q += (int64_t)gridDim.x * blockDim.x) {
+        float m = 0.f;
+        for (int64_t t = 0; t < ntri; ++t) {
+            const float2 v = K[q + nloc * t];
+            m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+        float sc;
+        if constexpr (KF == MR_KF_I16) sc = m > 0.f ? m / 32767.f : 1.f;
+        else sc = m > 0.f ? m : 1.f;
+        scale[q] = sc;
+        const float inv = 1.f / sc;
+        for (int64_t t = 0; t < ntri; ++t) {
+            const float2 v = K[q + nloc * t];
+            if constexpr (KF == MR_KF_I16) {
+                short2 c;
+                c.x = (short)__float2int_rn(fminf(fmaxf(v.x * inv, -32767.f), 32767.f));
+                c.y = (short)__float2int_rn(fminf(fmaxf(v.y * inv, -32767.f), 32767.f));
+                reinterpret_cast<short2 *>(out)[q + nloc * t] = c;
+            } else {
+                reinterpret_cast<__nv_bfloat162 *>(out)[q + nloc * t] =
+                    __floats2bfloat162_rn(v.x * inv, v.y * inv);
+            }
+        }
+    }
+}
+
+extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_complex64) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_set_kernel_format: op is NULL");
+    MR_REQUIRE(format == MR_B200_KF_COMPLEX64 || format == MR_B200_KF_BF16 ||
+                   format == MR_B200_KF_INT16,
+               "mr_b200_op_set_kernel_format: unknown format %d", format);
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
+    int rc = MR_SUCCESS;
+    cudaStream_t s = op->stream;
+    if (format == MR_B200_KF_COMPLEX64) {
+        if (!op->K) {
+            rc = MR_ERR_UNSUPPORTED;
+            mr_set_error("the complex64 kernel was released; it cannot be restored");
+        } else {
+            op->kf = MR_KF_F32;
+        }
+    } else if (!op->K) {
+        rc = MR_ERR_UNSUPPORTED;
+        mr_set_error("the complex64 kernel was released; it cannot be re-quantised");
+    } else {
+        const int64_t nloc = op->cfg.is_masked ? op->cfg.num_masked : mr_pad_size(&op->cfg);
+        const int64_t ntri = mr_num_tri(op->cfg.L);
+        if (op->K16) cudaFree(op->K16);
+        if (op->K16_scale) cudaFree(op->K16_scale);
+        op->K16 = nullptr;
+        op->K16_scale = nullptr;
+        if (cudaMalloc(&op->K16, (size_t)nloc * ntri * 4) != cudaSuccess ||
+            cudaMalloc(&op->K16_scale, (size_t)nloc * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError();
+            rc = MR_ERR_ALLOC;
+            mr_set_error("failed to allocate the 16-bit kernel");
+        } else {
+            const unsigned blocks = (unsigned)std::min<int64_t>(mr_cdiv(nloc, 256), 148 * 16);
+            if (format == MR_B200_KF_INT16)
+                k_quantize<MR_KF_I16><<<blocks, 256, 0, s>>>(op->K16, op->K16_scale, op->K, nloc, ntri);
+            else
+                k_quantize<MR_KF_BF16><<<blocks, 256, 0, s>>>(op->K16, op->K16_scale, op->K, nloc, ntri);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+                rc = MR_ERR_CUDA;
+                mr_set_error("kernel quantisation failed");
+            } else {
+                op->kf = format == MR_B200_KF_INT16 ? MR_KF_I16 : MR_KF_BF16;
+                if (!keep_complex64 && op->K_own) {
+                    cudaFree(op->K_own);
+                    op->K_own = nullptr;
+                    op->K = nullptr;
+                }
+            }
+        }
+    }
+    if (prev != op->dev) cudaSetDevice(prev);
+    return rc;
+}
+
+extern "C" int mr_b200_op_kernel_format(mr_op op, int *format) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && format != nullptr, "mr_b200_op_kernel_format: NULL argument");
+    *format = op->kf == MR_KF_F32 ? MR_B200_KF_COMPLEX64
+                                  : (op->kf == MR_KF_I16 ? MR_B200_KF_INT16 : MR_B200_KF_BF16);
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_b200_op_launches(mr_op op, int *n) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");
+    *n = mr_plan_launch_count(op->plan);
+    return MR_SUCCESS;
+}
