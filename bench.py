@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""Headline benchmark: A^H A applies/s of the Toeplitz operator.
+
+Workload (default ``stack320``): stack-of-stars golden-angle radial,
+image 320 x 320 x 56, grid 640 x 640 x 56, L = 16, 12 coils, 1000 spokes x
+640 readout points, Gram blocks from a random orthonormal 16 x 200 temporal
+basis (spokes split evenly over 200 frames), smoothed coil maps with
+sum |S_c|^2 = 1, x standard complex normal; all seeded synthetic data. One
+step = one apply ``op(x)`` of the operator built by ``create_op`` (kernel
+built on the GPU, complex64 unless ``--kernel-format`` says otherwise).
+
+Arms:
+* default: the CUDA library. ``value`` = applies/s with inputs resident on
+  the GPU (CUDA events on the operator's stream, K timed steps between a
+  barrier + synchronize on both sides, max over ranks); ``e2e`` = the same
+  metric through ``op(x)`` with host buffers, the host->device copy of x and
+  the device->host copy of A^H A x inside every step.
+* ``--impl reference``: the reference has no CPU implementation of the path
+  here (its CPU route, FINUFFT, is absent), so this times the FP32 CPU port of
+  the reference's apply (``oracle/cpu_port.py``) on all host cores; one step
+  is one coil's term of the apply (a bounded sample), scaled to applies/s.
+
+Several GPUs (torchrun): independent replicas, one operator per GPU, no
+collective on the data path (``scaling`` = weak).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "A^H A applies/s"
+UNIT = "applies/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="stack320")
+    ap.add_argument("--kernel-format", default="complex64",
+                    choices=["complex64", "bf16", "int16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-samples", type=int, default=2)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(name: str, wl: dict) -> dict:
+    return {"workload": name, "traj_type": wl["traj_type"], "n_dim": list(wl["n_dim"]),
+            "phi2_dim": list(wl["phi2_dim"]), "L": wl["L"], "n_coils": wl["n_coils"],
+            "Ntrajs": int(wl["traj"].shape[2]), "Nkx": int(wl["traj"].shape[1])}
+
+
+def alg_bytes(wl: dict, kbytes_per_elem: float, scale_bytes: int) -> dict:
+    """Algorithmic bytes per apply (3-pass pruned design) and of pass 3.
+
+    B_alg = 8 [Vimg L + Vimg C + 4 (Vpad/2) L C + Vimg C + Vimg L] + K,
+    K = kernel bytes; pass 3 (x transform + block multiply) reads and writes
+    the Mz*My*Nx intermediate of every plane and reads the kernel once.
+    """
+    n, m, L, C = wl["n_dim"], wl["phi2_dim"], wl["L"], wl["n_coils"]
+    vimg = n[0] * n[1] * n[2]
+    vpad = m[0] * m[1] * m[2]
+    ntri = L * (L + 1) // 2
+    K = vpad * ntri * kbytes_per_elem + (vpad * scale_bytes)
+    b_apply = 8 * (vimg * L + vimg * C + 4 * (vpad // 2) * L * C + vimg * C + vimg * L) + K
+    w1 = m[2] * m[1] * n[0] * L * C * 8
+    b_pass3 = 2 * w1 + K
+    return {"apply": float(b_apply), "x_blockdiag": float(b_pass3), "kernel": float(K)}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_index: int):
+        self.dev = dev_index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def committed_traffic(kernel_format: str):
+    """DRAM bytes per launch of pass 3 from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "x_blockdiag_stack320.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_launch", {}).get(kernel_format)
+    except Exception:
+        return None
+
+
+def cpu_baseline(wl: dict, samples: int) -> dict:
+    from oracle import aha_oracle as O
+    from oracle import cpu_port
+
+    shape = (O.num_tri(wl["L"]),) + O.spatial_axes(wl["traj_type"], wl["phi2_dim"])
+    cp = cpu_port.CpuToeplitz(wl["traj_type"], wl["n_dim"], wl["phi2_dim"], wl["L"],
+                              wl["SEs"], cpu_port.timing_kernel(shape), natural=True)
+    cp.apply_coil(wl["x"], 0)  # warm-up (FFT plans, page faults)
+    ts = []
+    for k in range(samples):
+        t0 = time.perf_counter()
+        cp.apply_coil(wl["x"], k % wl["n_coils"])
+        ts.append(time.perf_counter() - t0)
+    t = statistics.median(ts)
+    return {"value": 1.0 / (t * wl["n_coils"]), "unit": UNIT, "cores": cpu_port.cores(),
+            "kind": "port",
+            "sample": f"one coil's term of the apply (1 of {wl['n_coils']}), median of "
+                      f"{samples}, scaled x{wl['n_coils']}; FP32 scipy.fft + C/OpenMP block "
+                      f"multiply with a timing kernel of the full size"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from mr_aha_b200 import synth
+    from oracle import aha_oracle as O
+    from oracle import cpu_port
+
+    wl = synth.workload(args.workload)
+    ntri = O.num_tri(wl["L"])
+    shape = (ntri,) + O.spatial_axes(wl["traj_type"], wl["phi2_dim"])
+    cp = cpu_port.CpuToeplitz(wl["traj_type"], wl["n_dim"], wl["phi2_dim"], wl["L"],
+                              wl["SEs"], cpu_port.timing_kernel(shape), natural=True)
+    for k in range(args.warmup):
+        cp.apply_coil(wl["x"], k % wl["n_coils"])
+    ts = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        cp.apply_coil(wl["x"], k % wl["n_coils"])
+        ts.append(time.perf_counter() - t0)
+    per_apply = sum(ts) / len(ts) * wl["n_coils"]
+    v = 1.0 / per_apply
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sum(ts) / len(ts),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c64",
+            "data": "synthetic", "impl": "reference",
+            "config": workload_config(args.workload, wl),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cpu_port.cores(), "kind": "port",
+                             "sample": f"one coil's term per step (1 of {wl['n_coils']}), "
+                                       f"scaled x{wl['n_coils']}"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        dist = dist_mod
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import synth
+
+    wl = synth.workload(args.workload)
+    dev = torch.device("cuda", local)
+    t0 = time.perf_counter()
+    x_h = torch.from_numpy(wl["x"]).pin_memory()
+    x = x_h.to(dev)
+    S = torch.from_numpy(wl["SEs"]).to(dev)
+    phi2 = torch.from_numpy(wl["phi2"]).to(dev)
+    traj = torch.from_numpy(wl["traj"]).to(dev)
+    cfg = mr.make_config(wl["traj_type"], wl["n_dim"], wl["L"], phi2_dim=wl["phi2_dim"],
+                         n_coils=wl["n_coils"], mem_fraction=0.9)
+    op = mr.create_op(cfg, S, phi2, traj, kernel_format=args.kernel_format,
+                      keep_complex64=args.kernel_format == "complex64")
+    del phi2
+    info = op.info
+    setup_s = time.perf_counter() - t0
+    out = torch.empty_like(x)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        op(x, out=out)
+    torch.cuda.synchronize(dev)
+    prof = op.profile(x, out=out)
+    launches = op.launches_per_apply
+
+    # ---- device-resident timed region ----
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    sampler.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        op(x, out=out)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- end-to-end through op(x) with host buffers ----
+    y_h = torch.empty(x_h.shape, dtype=x_h.dtype).pin_memory()
+    xe = torch.empty_like(x)
+    for _ in range(2):
+        xe.copy_(x_h, non_blocking=True)
+        op(xe, out=out)
+        y_h.copy_(out, non_blocking=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0.record(stream)
+    for _ in range(args.steps):
+        xe.copy_(x_h, non_blocking=True)
+        op(xe, out=out)
+        y_h.copy_(out, non_blocking=True)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms_e = e0.elapsed_time(e1)
+    me = torch.tensor([ms_e], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(me, op=dist.ReduceOp.MAX)
+    ms_e = float(me.item())
+    e2e = {"value": world * args.steps / (ms_e / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(x_h.numel() * 8), "d2h_bytes_per_step": int(y_h.numel() * 8)}
+
+    # ---- roofline of the dominant kernel ----
+    kb = {"complex64": 8, "bf16": 4, "int16": 4}[args.kernel_format]
+    sb = 0 if args.kernel_format == "complex64" else 4
+    ab = alg_bytes(wl, kb, sb)
+    per_pass = {}
+    for name, t in prof:
+        per_pass[name] = per_pass.get(name, 0.0) + t
+    total_prof = sum(per_pass.values())
+    dom = max(per_pass, key=per_pass.get)
+    n_dom = sum(1 for name, _ in prof if name == dom)
+    dom_ms = per_pass[dom] / n_dom
+    peak, peak_kind = measured_peak_hbm()
+    dom_bytes = ab.get(dom)
+    roof = None
+    if dom_bytes is not None:
+        ngroups = max(1, n_dom)
+        achieved = (dom_bytes / ngroups) / (dom_ms / 1e3) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                "alg_bytes_per_launch": dom_bytes / ngroups,
+                "launch_ms": dom_ms, "traffic": committed_traffic(args.kernel_format)}
+    apply_ms = ms / args.steps
+    apply_roof = {"alg_bytes": ab["apply"], "achieved_gbs": ab["apply"] / (apply_ms / 1e3) / 1e9,
+                  "frac": ab["apply"] / (apply_ms / 1e3) / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline(wl, args.cpu_samples)
+        except Exception as exc:  # report, do not fail the bench line
+            cpu = {"value": None, "error": f"{type(exc).__name__}: {exc}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": apply_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64" if args.kernel_format == "complex64" else f"c64+{args.kernel_format}-kernel",
+            "data": "synthetic",
+            "config": dict(workload_config(args.workload, wl),
+                           kernel_format=args.kernel_format,
+                           parallelism=f"replicas{world}",
+                           l2="inputs larger than L2 (25 GB kernel streamed per apply)"),
+            "e2e": e2e,
+            "roofline": roof,
+            "apply_roofline": apply_roof,
+            "passes_ms": {k: round(v, 4) for k, v in per_pass.items()},
+            "profiled_apply_ms": total_prof,
+            "gpu_launches": launches * args.steps,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "setup_s": setup_s,
+            "toep_ms": info["toep_ms"],
+        }
+        print(json.dumps(line), flush=True)
+    op.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -29,6 +29,14 @@ MR_EXPORT int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_comple
 /* No reference counterpart. Current kernel format of the operator. */
 MR_EXPORT int mr_b200_op_kernel_format(mr_op op, int *format);
 
+/* No reference counterpart. One mr_op_execute with a CUDA event recorded on
+ * the operator's stream around every kernel: ms[k] is the time of launch k,
+ * names + 32*k its NUL-terminated pass name (names may be NULL). Synchronous.
+ * (Per-stage timing like the reference's MR_AHA_CUDA_PROFILE printout,
+ * src/cuda/mr_aha.cu:520-623, returned to the caller instead.) */
+MR_EXPORT int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_AhAx,
+                                 float *ms, char *names, int max_passes, int *n_passes);
+
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 

@@ -514,6 +514,23 @@ class AhAOp:
         check(lib.mr_b200_op_launches(self._handle, ctypes.byref(n)), "mr_b200_op_launches")
         return int(n.value)
 
+    def profile(self, x, out=None) -> list:
+        """One apply with CUDA events around every kernel on the operator's
+        stream: ``[(pass_name, ms), ...]`` in launch order (synchronous)."""
+        self._check_open()
+        if out is None:
+            out = _empty(tuple(x.shape), "complex64", _device_of(x))
+        nmax = 64
+        ms = (ctypes.c_float * nmax)()
+        names = ctypes.create_string_buffer(32 * nmax)
+        n = ctypes.c_int(0)
+        check(lib.mr_b200_op_profile(self._handle, _ptr(x, "x", "complex64"),
+                                     _ptr(out, "out", "complex64"), ms, names, nmax,
+                                     ctypes.byref(n)), "mr_b200_op_profile")
+        raw = names.raw
+        return [(raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(), float(ms[k]))
+                for k in range(n.value)]
+
     @property
     def info(self) -> dict:
         self._check_open()
@@ -544,7 +561,7 @@ class AhAOp:
         class _View:
             def __init__(self, p, n, owner):
                 self.__cuda_array_interface__ = {
-                    "shape": (n,), "typestr": "<c8", "data": (p, True), "version": 3,
+                    "shape": (n,), "typestr": "<c8", "data": (p, False), "version": 3,
                     "strides": None}
                 self._owner = owner
 

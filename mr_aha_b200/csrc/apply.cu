@@ -294,9 +294,19 @@ int mr_plan_launch_count(mr_aha_plan plan) { return plan->launches; }
 // Execution
 // ---------------------------------------------------------------------------
 
+static void prof_mark(mr_prof *prof, const char *name, cudaStream_t s) {
+    if (!prof || prof->n >= MR_PROF_MAX) return;
+    prof->name[prof->n] = name;
+    cudaEventRecord(prof->ev[++prof->n], s);
+}
+
 int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                       const mr_kernel_ref &K0, const int64_t *d_mask, float2 *out,
-                      cudaStream_t s) {
+                      cudaStream_t s, mr_prof *prof) {
+    if (prof) {
+        prof->n = 0;
+        cudaEventRecord(prof->ev[0], s);
+    }
     const mr_config &cfg = p->cfg;
     const mr_geom &g = p->g;
     const bool has_z = cfg.n_spatial == 3;
@@ -312,6 +322,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         MR_LAUNCH_CHECK("k_mask_inverse");
         K.inv = p->d_inv;
         K.stride = nm;
+        prof_mark(prof, "mask_inverse", s);
     } else {
         K.inv = nullptr;
         K.stride = g.vpad;
@@ -352,6 +363,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             a.scale = 1.f;
             rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
             if (rc != MR_SUCCESS) return rc;
+            prof_mark(prof, "z_forward", s);
         }
         // ---- pass 2: y lines, zero-pad along y ----
         {
@@ -389,6 +401,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
             }
             if (rc != MR_SUCCESS) return rc;
+            prof_mark(prof, "y_forward", s);
         }
         // ---- pass 3: x lines with the block multiply ----
         {
@@ -420,6 +433,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.K = K;
                 rc = mr_launch_xbd(a, s);
                 if (rc != MR_SUCCESS) return rc;
+                prof_mark(prof, "x_blockdiag", s);
             } else {
                 const int rows = 4;
                 a.rows_cta = rows;
@@ -434,8 +448,10 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.shift_out = 0;
                 rc = mr_launch_xplain(-1, a, s);
                 if (rc != MR_SUCCESS) return rc;
+                prof_mark(prof, "x_forward", s);
                 rc = launch_bd_full(p->W2, p->W3, g, K, G, s);
                 if (rc != MR_SUCCESS) return rc;
+                prof_mark(prof, "blockdiag", s);
                 a.src = p->W3;
                 a.dst = p->W1;
                 a.s_row = Mx;
@@ -446,6 +462,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.shift_out = g.cn[0];
                 rc = mr_launch_xplain(1, a, s);
                 if (rc != MR_SUCCESS) return rc;
+                prof_mark(prof, "x_inverse", s);
             }
         }
         // ---- pass 4: y lines back, crop ----
@@ -488,6 +505,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
             }
             if (rc != MR_SUCCESS) return rc;
+            prof_mark(prof, "y_inverse", s);
         }
         // ---- pass 5: z lines back, crop, conj(S_c) coil sum ----
         if (has_z) {
@@ -520,6 +538,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             a.scale = 1.f;
             rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
             if (rc != MR_SUCCESS) return rc;
+            prof_mark(prof, "z_inverse", s);
         }
     }
     if (cfg.verbose) {

@@ -85,9 +85,18 @@ int mr_smem_limit();
 
 // Plan helpers for internal callers --------------------------------------
 
+// Optional per-pass timing of one execute: an event is recorded on the
+// stream before the first and after every pass; pass names are static.
+#define MR_PROF_MAX 64
+struct mr_prof {
+    int n;                         // events recorded
+    cudaEvent_t ev[MR_PROF_MAX + 1];
+    const char *name[MR_PROF_MAX]; // pass ending at event k + 1
+};
+
 int mr_plan_execute_k(mr_aha_plan plan, const float2 *x, const float2 *S,
                       const mr_kernel_ref &K, const int64_t *d_mask, float2 *out,
-                      cudaStream_t s);
+                      cudaStream_t s, mr_prof *prof = nullptr);
 int mr_plan_kf_supported(mr_aha_plan plan);
 int mr_plan_group(mr_aha_plan plan);
 cudaStream_t mr_plan_stream(mr_aha_plan plan);

@@ -411,6 +411,46 @@ extern "C" int mr_b200_op_kernel_format(mr_op op, int *format) {
     return MR_SUCCESS;
 }
 
+extern "C" int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_AhAx,
+                                  float *ms, char *names, int max_passes, int *n_passes) {
+    mr_clear_error();
+    MR_REQUIRE(op && d_x && d_AhAx && ms && n_passes, "mr_b200_op_profile: NULL argument");
+    MR_REQUIRE(max_passes >= 1, "mr_b200_op_profile: max_passes must be >= 1");
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
+    mr_prof prof;
+    std::memset(&prof, 0, sizeof(prof));
+    int rc = MR_SUCCESS;
+    for (int k = 0; k <= MR_PROF_MAX; ++k)
+        if (cudaEventCreate(&prof.ev[k]) != cudaSuccess) rc = MR_ERR_CUDA;
+    if (rc == MR_SUCCESS)
+        rc = mr_plan_execute_k(op->plan, reinterpret_cast<const float2 *>(d_x), op->S,
+                               op_kernel_ref(op), op->mask, reinterpret_cast<float2 *>(d_AhAx),
+                               op->stream, &prof);
+    if (rc == MR_SUCCESS && cudaStreamSynchronize(op->stream) != cudaSuccess) {
+        rc = MR_ERR_CUDA;
+        mr_set_error("profiled execute failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    if (rc == MR_SUCCESS) {
+        const int n = std::min(prof.n, max_passes);
+        for (int k = 0; k < n; ++k) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, prof.ev[k], prof.ev[k + 1]);
+            ms[k] = t;
+            if (names) {
+                std::strncpy(names + 32 * k, prof.name[k], 31);
+                names[32 * k + 31] = '\0';
+            }
+        }
+        *n_passes = n;
+    }
+    for (int k = 0; k <= MR_PROF_MAX; ++k)
+        if (prof.ev[k]) cudaEventDestroy(prof.ev[k]);
+    if (prev != op->dev) cudaSetDevice(prev);
+    return rc;
+}
+
 extern "C" int mr_b200_op_launches(mr_op op, int *n) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");
