@@ -40,6 +40,25 @@ MR_EXPORT int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 
+/* Size of the library's static device scratch array used by
+ * mr_b200_aha_toeplitz_noalloc (reserved on every GPU that loads the
+ * library, until the process exits). */
+#define MR_B200_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* No counterpart in the reference. The same result as mr_aha_toeplitz
+ * (same arguments), for callers that cannot allocate device memory: its work
+ * buffers and FFT tables come from the library's static scratch array
+ * (MR_B200_NOALLOC_SCRATCH_BYTES per GPU) instead of cudaMalloc, and it
+ * calls no allocation routine. Problems whose work space does not fit even
+ * one coil at a time return MR_ERR_UNSUPPORTED. Asynchronous on cfg->stream.
+ * All calls share the array: calls that overlap on the GPU race. The first
+ * call on a device looks up the array's device address there; make it
+ * before any stream capture. */
+MR_EXPORT int mr_b200_aha_toeplitz_noalloc(const mr_config *cfg, const mr_complex *d_x,
+                                           const mr_complex *d_SEs,
+                                           const mr_complex *d_phi2_toep,
+                                           const int64_t *d_mask, mr_complex *d_AhAx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -592,3 +592,103 @@ extern "C" int mr_aha_toeplitz(const mr_config *cfg, const mr_complex *d_x,
     const int rc2 = mr_aha_plan_destroy(plan);
     return rc != MR_SUCCESS ? rc : rc2;
 }
+
+// ---------------------------------------------------------------------------
+// Plan over caller-provided device scratch (used by the allocation-free
+// entry point in noalloc.cu; nothing here allocates device memory)
+// ---------------------------------------------------------------------------
+
+// W_M^e = exp(-2 pi i e / M) for the three axes, into one table.
+__global__ void k_twiddle_table(float2 *tw, int m0, int m1, int m2) {
+    const int total = m0 + m1 + m2;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        int M = m0, k = e;
+        if (k >= m0) {
+            k -= m0;
+            M = m1;
+            if (k >= m1) {
+                k -= m1;
+                M = m2;
+            }
+        }
+        double s, c;
+        sincospi(-2.0 * (double)k / (double)M, &s, &c);
+        tw[e] = make_float2((float)c, (float)s);
+    }
+}
+
+size_t mr_plan_struct_size() { return sizeof(struct mr_aha_plan_s); }
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, void *storage,
+                             size_t *needed) {
+    int rc = mr_config_validate(cfg);
+    if (rc != MR_SUCCESS) return rc;
+    mr_aha_plan p = (mr_aha_plan)storage;
+    std::memset(p, 0, sizeof(*p));
+    p->cfg = *cfg;
+    p->stream = (cudaStream_t)cfg->stream;
+    mr_geom_from_config(cfg, &p->g);
+    const mr_geom &g = p->g;
+    for (int d = 0; d < 3; ++d) {
+        rc = mr_fft_factor(g.m[d], &p->ax[d]);
+        if (rc != MR_SUCCESS) return rc;
+    }
+    const size_t lim = (size_t)mr_smem_limit();
+    p->xt_z = mr_pick_xt(g.m[2], g.m[2], MR_SM_COILSUM, g.n[0], lim / 2);
+    p->xt_y = mr_pick_xt(g.m[1], g.m[1], MR_SM_COILSUM, g.n[0], lim / 2);
+    if (mr_strided_smem(g.m[2], p->xt_z, g.m[2], MR_SM_COILSUM) > lim ||
+        mr_strided_smem(g.m[1], p->xt_y, g.m[1], MR_SM_COILSUM) > lim)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d / %d points exceeds shared memory",
+                g.m[1], g.m[2]);
+    p->nc_cta = 1;
+    p->fused = mr_xbd_smem(g.m[0], g.L, 1) <= lim;
+    if (p->fused && g.L <= 16 && mr_xbd_smem(g.m[0], g.L, 2) <= lim && cfg->n_coils >= 2)
+        p->nc_cta = 2;
+    if (!p->fused && mr_xplain_smem(g.m[0], 1) > lim)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d points exceeds shared memory", g.m[0]);
+    // Layout: twiddles | inverse mask map | W0 | W1 | W2 | W3, each 256-byte aligned.
+    const bool has_z = cfg->n_spatial == 3;
+    const size_t tw_b = align256((size_t)(g.m[0] + g.m[1] + g.m[2]) * sizeof(float2));
+    const size_t inv_b = cfg->is_masked ? align256((size_t)g.vpad * sizeof(int)) : 0;
+    int group = cfg->n_coils;
+    size_t w0_b = 0, w1_b = 0, wf_b = 0, total = 0;
+    for (;; --group) {
+        const size_t P = (size_t)group * g.L;
+        w0_b = has_z ? align256(P * g.m[2] * g.n[1] * g.n[0] * sizeof(float2)) : 0;
+        w1_b = align256(P * g.m[2] * g.m[1] * g.n[0] * sizeof(float2));
+        wf_b = p->fused ? 0 : align256(P * (size_t)g.vpad * sizeof(float2));
+        total = tw_b + inv_b + w0_b + w1_b + 2 * wf_b;
+        if (total <= bytes || group == 1) break;
+    }
+    if (needed) *needed = total;
+    if (total > bytes)
+        MR_FAIL(MR_ERR_UNSUPPORTED,
+                "this operator needs %zu bytes of work space even one coil at a time, more "
+                "than the %zu bytes of the library's static scratch array",
+                total, bytes);
+    char *q = scratch;
+    p->d_tw = (float2 *)q;
+    q += tw_b;
+    p->d_inv = cfg->is_masked ? (int *)q : nullptr;
+    q += inv_b;
+    p->W0 = has_z ? (float2 *)q : nullptr;
+    q += w0_b;
+    p->W1 = (float2 *)q;
+    q += w1_b;
+    p->W2 = p->fused ? nullptr : (float2 *)q;
+    q += wf_b;
+    p->W3 = p->fused ? nullptr : (float2 *)q;
+    p->group = group;
+    p->ax[0].tw = p->d_tw;
+    p->ax[1].tw = p->d_tw + g.m[0];
+    p->ax[2].tw = p->d_tw + g.m[0] + g.m[1];
+    k_twiddle_table<<<(unsigned)mr_cdiv(g.m[0] + g.m[1] + g.m[2], 256), 256, 0, p->stream>>>(
+        p->d_tw, g.m[0], g.m[1], g.m[2]);
+    MR_LAUNCH_CHECK("k_twiddle_table");
+    const int ngroups = (int)mr_cdiv(cfg->n_coils, group);
+    const int per = (has_z ? 2 : 0) + 2 + (p->fused ? 1 : 3);
+    p->launches = ngroups * per + (cfg->is_masked ? 1 : 0) + 1;
+    return MR_SUCCESS;
+}

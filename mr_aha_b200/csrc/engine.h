@@ -102,3 +102,12 @@ int mr_plan_group(mr_aha_plan plan);
 cudaStream_t mr_plan_stream(mr_aha_plan plan);
 // Number of kernels one execute launches (for accounting).
 int mr_plan_launch_count(mr_aha_plan plan);
+
+// Plan over caller-provided device scratch: fills `storage` (at least
+// mr_plan_struct_size() bytes, host memory) with a plan whose work buffers
+// and FFT tables live in [scratch, scratch + bytes); launches the twiddle
+// table kernel on cfg->stream; allocates nothing. *needed receives the
+// bytes the chosen coil group uses.
+size_t mr_plan_struct_size();
+int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, void *storage,
+                             size_t *needed);
