@@ -41,8 +41,41 @@ struct mr_aha_plan_s {
     int fused;       // pass 3 with the block multiply inside
     int nc_cta;      // coils per CTA in the fused pass 3
     int xt_z, xt_y;  // strided tile widths
+    // in-place kernels (passes2.cu): tile exponents per (axis, store mode),
+    // -1 when unavailable; coils per block-diagonal tile, 0 when unavailable
+    int xts_z_buf, xts_z_cs, xts_y_buf, xts_y_cs;
+    int nc2;
+    // compile-time-specialised kernels (passes3.cu): tile widths, 0 if none
+    int xt3_z_buf, xt3_z_cs, xt3_y_buf, xt3_y_cs;
+    int nc3;
     int launches;    // kernels per execute (accounting)
 };
+
+// Choose the in-place kernels where the lengths allow them.
+static void plan_pick_v2(mr_aha_plan p, size_t lim) {
+    const mr_geom &g = p->g;
+    const bool off = mr_env_int("MR_AHA_B200_FFT_V1", 0) != 0;
+    p->xts_z_buf = p->xts_z_cs = p->xts_y_buf = p->xts_y_cs = -1;
+    p->nc2 = 0;
+    if (off) return;
+    if (p->ax[2].small) {
+        p->xts_z_buf = mr_strided2_xts(g.m[2], g.m[2], MR_SM_BUF, g.n[0], lim);
+        p->xts_z_cs = mr_strided2_xts(g.m[2], g.n[2], MR_SM_COILSUM, g.n[0], lim);
+    }
+    if (p->ax[1].small) {
+        p->xts_y_buf = mr_strided2_xts(g.m[1], g.m[1], MR_SM_BUF, g.n[0], lim);
+        p->xts_y_cs = mr_strided2_xts(g.m[1], g.n[1], MR_SM_COILSUM, g.n[0], lim);
+    }
+    if (p->ax[0].small && p->fused) p->nc2 = mr_xbd2_coils(g.m[0], g.L, p->cfg.n_coils, lim);
+    p->xt3_z_buf = p->xt3_z_cs = p->xt3_y_buf = p->xt3_y_cs = 0;
+    p->nc3 = 0;
+    if (mr_env_int("MR_AHA_B200_NO_FIXED", 0)) return;
+    p->xt3_z_buf = mr_fixed_strided_xt(g.m[2], MR_SM_BUF);
+    p->xt3_z_cs = mr_fixed_strided_xt(g.m[2], MR_SM_COILSUM);
+    p->xt3_y_buf = mr_fixed_strided_xt(g.m[1], MR_SM_BUF);
+    p->xt3_y_cs = mr_fixed_strided_xt(g.m[1], MR_SM_COILSUM);
+    if (p->fused) p->nc3 = mr_fixed_xbd_coils(g.m[0], g.L);
+}
 
 // ---------------------------------------------------------------------------
 // Stand-alone block multiply over a full-grid buffer (unfused pass 3)
@@ -231,6 +264,7 @@ static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
         MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d points exceeds shared memory", g.m[0]);
     }
     if (mr_env_int("MR_AHA_B200_UNFUSED_BD", 0)) p->fused = 0;
+    plan_pick_v2(p, lim);
 
     // Coil group: all coils if they fit the budget, else fewer.
     size_t budget = 0;
@@ -294,6 +328,25 @@ int mr_plan_launch_count(mr_aha_plan plan) { return plan->launches; }
 // Execution
 // ---------------------------------------------------------------------------
 
+// Strided pass with the in-place kernel when available (xts >= 0), else the
+// ping-pong kernel with tile width xt_v1.
+static int launch_strided_auto(int dir, int lm, int sm, mr_strided_args a, int xts, int xt_v1,
+                               cudaStream_t s, int xt3 = 0) {
+    if (xt3 > 0) {
+        a.xt = xt3;
+        a.nxt = (int)mr_cdiv(a.nfast, a.xt);
+        return mr_launch_strided3(dir, lm, sm, a, s);
+    }
+    if (xts >= 0) {
+        a.xt = 1 << xts;
+        a.nxt = (int)mr_cdiv(a.nfast, a.xt);
+        return mr_launch_strided2(dir, lm, sm, a, xts, s);
+    }
+    a.xt = xt_v1;
+    a.nxt = (int)mr_cdiv(a.nfast, a.xt);
+    return mr_launch_strided(dir, lm, sm, a, s);
+}
+
 static void prof_mark(mr_prof *prof, const char *name, cudaStream_t s) {
     if (!prof || prof->n >= MR_PROF_MAX) return;
     prof->name[prof->n] = name;
@@ -339,13 +392,13 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         if (has_z) {
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
+            // z lines: the (y, x) plane is contiguous, so tiles run over the
+            // flattened plane index
             a.ax = p->ax[2];
-            a.nfast = Nx;
-            a.xt = p->xt_z;
-            a.nxt = (int)mr_cdiv(Nx, a.xt);
-            a.nouter = Ny;
+            a.nfast = Nx * Ny;
+            a.nouter = 1;
             a.nplane = P;
-            a.s_outer = Nx;
+            a.s_outer = 0;
             a.s_axis = (int64_t)Nx * Ny;
             a.n_in = Nz;
             a.shift_in = g.cn[2];
@@ -356,12 +409,13 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             a.coil0 = c0;
             a.dst = p->W0;
             a.d_plane = w0_plane;
-            a.d_outer = Nx;
+            a.d_outer = 0;
             a.d_axis = (int64_t)Ny * Nx;
             a.n_out = Mz;
             a.shift_out = 0;
             a.scale = 1.f;
-            rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
+            rc = launch_strided_auto(-1, MR_LM_XS, MR_SM_BUF, a, p->xts_z_buf, p->xt_z, s,
+                                     p->xt3_z_buf);
             if (rc != MR_SUCCESS) return rc;
             prof_mark(prof, "z_forward", s);
         }
@@ -392,13 +446,15 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.s_plane = w0_plane;
                 a.s_outer = (int64_t)Ny * Nx;
                 a.s_axis = Nx;
-                rc = mr_launch_strided(-1, MR_LM_BUF, MR_SM_BUF, a, s);
+                rc = launch_strided_auto(-1, MR_LM_BUF, MR_SM_BUF, a, p->xts_y_buf, p->xt_y, s,
+                                         p->xt3_y_buf);
             } else {
                 a.xs_x = x;
                 a.xs_s = S;
                 a.s_outer = 0;
                 a.s_axis = Nx;
-                rc = mr_launch_strided(-1, MR_LM_XS, MR_SM_BUF, a, s);
+                rc = launch_strided_auto(-1, MR_LM_XS, MR_SM_BUF, a, p->xts_y_buf, p->xt_y, s,
+                                         p->xt3_y_buf);
             }
             if (rc != MR_SUCCESS) return rc;
             prof_mark(prof, "y_forward", s);
@@ -431,7 +487,17 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.cmy = g.cm[1];
                 a.cmz = g.cm[2];
                 a.K = K;
-                rc = mr_launch_xbd(a, s);
+                if (p->nc3 > 0) {
+                    a.nc = p->nc3;
+                    a.nchunk = (int)mr_cdiv(G, a.nc);
+                    rc = mr_launch_xbd3(a, s);
+                } else if (p->nc2 > 0) {
+                    a.nc = p->nc2;
+                    a.nchunk = (int)mr_cdiv(G, a.nc);
+                    rc = mr_launch_xbd2(a, s);
+                } else {
+                    rc = mr_launch_xbd(a, s);
+                }
                 if (rc != MR_SUCCESS) return rc;
                 prof_mark(prof, "x_blockdiag", s);
             } else {
@@ -492,7 +558,8 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.d_plane = w0_plane;
                 a.d_outer = (int64_t)Ny * Nx;
                 a.d_axis = Nx;
-                rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_BUF, a, s);
+                rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_BUF, a, p->xts_y_buf, p->xt_y, s,
+                                         p->xt3_y_buf);
             } else {
                 a.nplane = g.L;
                 a.xs_s = S;
@@ -502,7 +569,8 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.d_axis = Nx;
                 a.ncoil = G;
                 a.accumulate = accumulate;
-                rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
+                rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_COILSUM, a, p->xts_y_cs, p->xt_y, s,
+                                         p->xt3_y_cs);
             }
             if (rc != MR_SUCCESS) return rc;
             prof_mark(prof, "y_inverse", s);
@@ -512,14 +580,12 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
             a.ax = p->ax[2];
-            a.nfast = Nx;
-            a.xt = p->xt_z;
-            a.nxt = (int)mr_cdiv(Nx, a.xt);
-            a.nouter = Ny;
+            a.nfast = Nx * Ny;
+            a.nouter = 1;
             a.nplane = g.L;
             a.src = p->W0;
             a.s_plane = w0_plane;
-            a.s_outer = Nx;
+            a.s_outer = 0;
             a.s_axis = (int64_t)Ny * Nx;
             a.n_in = Mz;
             a.shift_in = 0;
@@ -531,12 +597,13 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             a.img_plane = g.vimg;
             a.dst = out;
             a.d_plane = g.vimg;
-            a.d_outer = Nx;
+            a.d_outer = 0;
             a.d_axis = (int64_t)Ny * Nx;
             a.ncoil = G;
             a.accumulate = accumulate;
             a.scale = 1.f;
-            rc = mr_launch_strided(1, MR_LM_BUF, MR_SM_COILSUM, a, s);
+            rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_COILSUM, a, p->xts_z_cs, p->xt_z, s,
+                                     p->xt3_z_cs);
             if (rc != MR_SUCCESS) return rc;
             prof_mark(prof, "z_inverse", s);
         }
@@ -648,6 +715,7 @@ int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, 
         p->nc_cta = 2;
     if (!p->fused && mr_xplain_smem(g.m[0], 1) > lim)
         MR_FAIL(MR_ERR_UNSUPPORTED, "an FFT line of %d points exceeds shared memory", g.m[0]);
+    plan_pick_v2(p, lim);
     // Layout: twiddles | inverse mask map | W0 | W1 | W2 | W3, each 256-byte aligned.
     const bool has_z = cfg->n_spatial == 3;
     const size_t tw_b = align256((size_t)(g.m[0] + g.m[1] + g.m[2]) * sizeof(float2));

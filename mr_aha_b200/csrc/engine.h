@@ -69,6 +69,23 @@ struct mr_x_args {
 
 int mr_launch_strided(int dir, int lmode, int smode, const mr_strided_args &a,
                       cudaStream_t s);
+// In-place register-staged variants (passes2.cu) for lengths whose radices
+// are all in {2, 3, 4, 5, 7, 8}: tile width 2^xts (from mr_strided2_xts, -1
+// if none fits) and nc coils per block-diagonal tile (mr_xbd2_coils, 0 if
+// none fits or L > 16).
+int mr_launch_strided2(int dir, int lmode, int smode, const mr_strided_args &a, int xts,
+                       cudaStream_t s);
+int mr_launch_xbd2(const mr_x_args &a, cudaStream_t s);
+int mr_strided2_xts(int M, int n_out, int smode, int nfast, size_t limit);
+// Compile-time-specialised variants (passes3.cu): widest instantiated tile for
+// a length and store mode (0 if none), coils per tile of the instantiated
+// block-diagonal pass for (M, L) (0 if none).
+int mr_fixed_strided_xt(int M, int smode);
+int mr_launch_strided3(int dir, int lmode, int smode, const mr_strided_args &a, cudaStream_t s);
+int mr_fixed_xbd_coils(int M, int L);
+int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s);
+int mr_xbd2_coils(int M, int L, int ncoil, size_t limit);
+int mr_xbd2_stride(int M);
 int mr_launch_xplain(int dir, const mr_x_args &a, cudaStream_t s);
 int mr_launch_xbd(const mr_x_args &a, cudaStream_t s);
 

@@ -17,10 +17,35 @@
 #define MR_FFT_MAX_PASSES 24
 #define MR_FFT_MAX_GENERIC_RADIX 256
 
+// Division by an invariant 32-bit divisor d >= 1 for dividends n < 2^31:
+// n / d = (umulhi(n, m) + n) >> s with s = ceil(log2 d) and
+// m = floor(2^32 (2^s - d) / d) + 1 (Granlund and Montgomery, "Division by
+// invariant integers using multiplication", PLDI 1994).
+struct mr_fdiv {
+    unsigned d, m, s;
+};
+
+__host__ __device__ inline mr_fdiv mr_make_fdiv(unsigned d) {
+    mr_fdiv f;
+    f.d = d;
+    unsigned s = 0;
+    while ((1ull << s) < (unsigned long long)d) ++s;
+    f.s = s;
+    f.m = (unsigned)((((unsigned long long)1 << 32) * ((1ull << s) - d)) / d + 1);
+    return f;
+}
+
+__device__ __forceinline__ int mr_div(int n, const mr_fdiv &f) {
+    return (int)((__umulhi((unsigned)n, f.m) + (unsigned)n) >> f.s);
+}
+
 struct mr_fft_axis {
     int M;
     int npass;
     int radix[MR_FFT_MAX_PASSES];
+    int p[MR_FFT_MAX_PASSES];        // product of the radices before pass s
+    mr_fdiv fp[MR_FFT_MAX_PASSES];   // division by p[s]
+    int small;                       // every radix in {2, 3, 4, 5, 7, 8}
     const float2 *tw;  // W_M^e = exp(-2 pi i e / M)
 };
 

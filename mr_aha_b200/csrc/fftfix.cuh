@@ -1,0 +1,129 @@
+// Compile-time-specialised in-place Stockham FFT for the lengths the plans
+// use most. The length, radix sequence, line count, strides and thread count
+// are template parameters, so every index of every butterfly folds to a
+// per-thread base plus constant offsets, and the passes contain no run-time
+// radix switch and (when the work divides evenly) no bounds guards. Same
+// formulation as fft_device.cuh: butterfly i of a radix-R pass with p =
+// product of earlier radices reads x[i + t M/R], twiddles by
+// W_{pR}^{t (i mod p)}, transforms, and writes y[(i - i mod p) R + i mod p + t p];
+// all reads of a pass finish (barrier) before its writes, in place.
+#pragma once
+
+#include "fft_device.cuh"
+
+namespace mrfix {
+
+struct radix_list {
+    int n;
+    int r[16];
+};
+
+// Radix policy of the host planner (passes.cu mr_fft_factor): eights, then a
+// four or a two, then fives, threes, sevens. Lengths with other factors are
+// not specialised (n = 0).
+constexpr radix_list factor(int M) {
+    radix_list l{0, {}};
+    int e2 = 0;
+    while (M % 2 == 0) {
+        M /= 2;
+        ++e2;
+    }
+    while (e2 >= 3) {
+        l.r[l.n++] = 8;
+        e2 -= 3;
+    }
+    if (e2 == 2) l.r[l.n++] = 4;
+    if (e2 == 1) l.r[l.n++] = 2;
+    while (M % 5 == 0) {
+        l.r[l.n++] = 5;
+        M /= 5;
+    }
+    while (M % 3 == 0) {
+        l.r[l.n++] = 3;
+        M /= 3;
+    }
+    while (M % 7 == 0) {
+        l.r[l.n++] = 7;
+        M /= 7;
+    }
+    if (M != 1) l.n = 0;
+    return l;
+}
+
+constexpr int max_stage(int M, int NL, int NT) {
+    const radix_list l = factor(M);
+    int m = 0;
+    for (int s = 0; s < l.n; ++s) {
+        const int R = l.r[s];
+        const int total = NL * (M / R);
+        const int nb = (total + NT - 1) / NT;
+        if (nb * R > m) m = nb * R;
+    }
+    return m;
+}
+
+template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int UA>
+__device__ __forceinline__ void pass(float2 *buf, const float2 *__restrict__ tw, float2 (&u)[UA]) {
+    constexpr int MR = M / R;
+    constexpr int TOTAL = NL * MR;
+    constexpr int NB = (TOTAL + NT - 1) / NT;
+    constexpr int TSTEP = M / (P * R);
+    constexpr bool EXACT = (TOTAL % NT) == 0;
+    static_assert(NB * R <= UA, "register stage too small");
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int w = tid + k * NT;
+        if (EXACT || w < TOTAL) {
+            const int i = w / NL;
+            const int b = w - i * NL;
+            const float2 *s = buf + b * LS + i * ES;
+#pragma unroll
+            for (int t = 0; t < R; ++t) u[k * R + t] = s[t * MR * ES];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int w = tid + k * NT;
+        if (EXACT || w < TOTAL) {
+            const int i = w / NL;
+            const int b = w - i * NL;
+            const int kk = i % P;
+            const int q = i / P;
+            if constexpr (P > 1) {
+                const int e1 = kk * TSTEP;
+#pragma unroll
+                for (int t = 1; t < R; ++t)
+                    u[k * R + t] = c_mul(u[k * R + t], tw_get<DIR>(tw, t * e1));
+            }
+            dft_small<R, DIR>(&u[k * R]);
+            float2 *d = buf + b * LS + (q * P * R + kk) * ES;
+#pragma unroll
+            for (int t = 0; t < R; ++t) d[t * P * ES] = u[k * R + t];
+        }
+    }
+    __syncthreads();
+}
+
+template <int DIR, int M, int NL, int ES, int LS, int NT, int S, int P, int UA>
+__device__ __forceinline__ void run(float2 *buf, const float2 *tw, float2 (&u)[UA]) {
+    constexpr radix_list l = factor(M);
+    if constexpr (S < l.n) {
+        constexpr int R = l.r[S];
+        pass<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u);
+        run<DIR, M, NL, ES, LS, NT, S + 1, P * R>(buf, tw, u);
+    }
+}
+
+// In-place transform of NL lines of length M held in shared memory (element
+// e of line b at buf[b * LS + e * ES]) by NT threads.
+template <int DIR, int M, int NL, int ES, int LS, int NT>
+__device__ __forceinline__ void fft(float2 *buf, const float2 *tw) {
+    static_assert(factor(M).n > 0, "length not specialised");
+    constexpr int UA = max_stage(M, NL, NT);
+    float2 u[UA];
+    run<DIR, M, NL, ES, LS, NT, 0, 1>(buf, tw, u);
+}
+
+}  // namespace mrfix

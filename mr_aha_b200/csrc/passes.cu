@@ -59,6 +59,15 @@ int mr_fft_factor(int M, mr_fft_axis *ax) {
         MR_FAIL(MR_ERR_UNSUPPORTED,
                 "FFT length %d has a prime factor %d above the supported %d", M, n,
                 MR_FFT_MAX_GENERIC_RADIX);
+    int prod = 1;
+    ax->small = 1;
+    for (int s = 0; s < ax->npass; ++s) {
+        ax->p[s] = prod;
+        ax->fp[s] = mr_make_fdiv((unsigned)prod);
+        const int r = ax->radix[s];
+        if (!(r == 2 || r == 3 || r == 4 || r == 5 || r == 7 || r == 8)) ax->small = 0;
+        prod *= r;
+    }
     return MR_SUCCESS;
 }
 

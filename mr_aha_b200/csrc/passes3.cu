@@ -1,0 +1,257 @@
+// Passes with a compile-time-specialised FFT (fftfix.cuh) for the common
+// lengths of the plans: the same data flow as the in-place kernels of
+// passes2.cu, with the transform length, tile width / coil count and rank as
+// template parameters. The plan uses these kernels when its geometry matches
+// an instantiated configuration (mr_fixed_*), else the generic ones.
+#include "engine.h"
+#include "fftfix.cuh"
+
+namespace {
+
+constexpr int kNT = 512;
+
+template <int DIR, int LM, int SM, int M, int XT>
+__global__ void __launch_bounds__(kNT) k_strided3(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int TILE = M * XT;
+    float2 *acc = sm + TILE;
+    int64_t bid = blockIdx.x;
+    const int plane = (int)(bid % a.nplane);
+    bid /= a.nplane;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int ncl = (SM == MR_SM_COILSUM) ? a.ncoil : 1;
+    const int64_t off0 = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
+    for (int cc = 0; cc < ncl; ++cc) {
+        const int sp = (SM == MR_SM_COILSUM) ? cc * a.L + plane : plane;
+        const float2 *srcp = nullptr, *xp = nullptr, *sp_s = nullptr;
+        if constexpr (LM == MR_LM_BUF) {
+            srcp = a.src + (int64_t)sp * a.s_plane + off0;
+        } else {
+            xp = a.xs_x + (int64_t)(sp % a.L) * a.img_plane + off0;
+            sp_s = a.xs_s + (int64_t)(a.coil0 + sp / a.L) * a.img_plane + off0;
+        }
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < TILE; idx += kNT) {
+            const int j = idx / XT;
+            const int xx = idx % XT;
+            int sa = j + a.shift_in;
+            if (sa >= M) sa -= M;
+            float2 v = make_float2(0.f, 0.f);
+            if (xx < nx && sa < a.n_in) {
+                const int64_t o = (int64_t)sa * a.s_axis + xx;
+                if constexpr (LM == MR_LM_BUF) v = srcp[o];
+                else v = c_mul(__ldg(sp_s + o), __ldg(xp + o));
+            }
+            sm[idx] = v;
+        }
+        __syncthreads();
+        mrfix::fft<DIR, M, XT, XT, 1, kNT>(sm, a.ax.tw);
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < a.n_out * XT; idx += kNT) {
+            const int da = idx / XT;
+            const int xx = idx % XT;
+            int q = da - a.shift_out;
+            if (q < 0) q += M;
+            const float2 v = sm[q * XT + xx];
+            if constexpr (SM == MR_SM_BUF) {
+                if (xx < nx)
+                    a.dst[(int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + xx] =
+                        c_scale(v, a.scale);
+            } else {
+                float2 w = make_float2(0.f, 0.f);
+                if (xx < nx)
+                    w = c_mulc(__ldg(a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0 +
+                                     (int64_t)da * a.d_axis + xx),
+                               v);
+                acc[idx] = (cc == 0) ? w : c_add(acc[idx], w);
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (SM == MR_SM_COILSUM) {
+        for (int idx = threadIdx.x; idx < a.n_out * XT; idx += kNT) {
+            const int da = idx / XT;
+            const int xx = idx % XT;
+            if (xx < nx) {
+                float2 *o = a.dst + (int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + xx;
+                const float2 v = c_scale(acc[idx], a.scale);
+                *o = a.accumulate ? c_add(*o, v) : v;
+            }
+        }
+    }
+}
+
+template <int M>
+constexpr int odd_stride() {
+    return (M % 2 == 0) ? M + 1 : M + 2;
+}
+
+template <int M, int L, int NC, int KF>
+__global__ void __launch_bounds__(kNT) k_xbd3(const __grid_constant__ mr_x_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int LS = odd_stride<M>();
+    constexpr int NL = NC * L;
+    const int chunk = (int)(blockIdx.x % a.nchunk);
+    const int loc = (int)(blockIdx.x / a.nchunk);
+    const int jy = loc % a.My;
+    const int jz = loc / a.My;
+    const int c0 = chunk * NC;
+    const int ncoils = min(NC, a.ncoil - c0);
+    const int64_t pbase = (int64_t)c0 * L;
+    const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
+    const int64_t rstride = a.plane_rows * a.s_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < NL * M; idx += kNT) {
+        const int b = idx / M;
+        const int j = idx - b * M;
+        int sa = j + a.shift_in;
+        if (sa >= M) sa -= M;
+        float2 v = make_float2(0.f, 0.f);
+        if (b < ncoils * L && sa < a.n_in) v = src[b * rstride + sa];
+        sm[b * LS + j] = v;
+    }
+    __syncthreads();
+    mrfix::fft<-1, M, NL, 1, LS, kNT>(sm, a.ax.tw);
+    const int ky = mr_nat2cent_d(jy, a.My, a.cmy);
+    const int kz = mr_nat2cent_d(jz, a.Mz, a.cmz);
+    constexpr int GW = 32 / NC;
+    constexpr int ITEMS = NC * ((M + GW - 1) / GW) * GW;
+    for (int w = threadIdx.x; w < ITEMS; w += kNT) {
+        const int lane = w & 31;
+        const int k = lane / GW;
+        const int jx = (w >> 5) * GW + (lane - k * GW);
+        if (jx >= M || k >= ncoils) continue;
+        float2 v[1][L], y[1][L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[0][l] = sm[(k * L + l) * LS + jx];
+        bool zero = false;
+        int64_t row;
+        if (a.K.inv) {
+            const int r = __ldg(a.K.inv + jx + (int64_t)M * (jy + (int64_t)a.My * jz));
+            zero = r < 0;
+            row = zero ? 0 : r;
+        } else {
+            row = mr_nat2cent_d(jx, M, a.cmx) + (int64_t)M * (ky + (int64_t)a.My * kz);
+        }
+        if (zero) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
+        } else {
+            const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
+            bd_block<L, 1, KF>(v, y, kl, a.upper);
+        }
+#pragma unroll
+        for (int l = 0; l < L; ++l) sm[(k * L + l) * LS + jx] = y[0][l];
+    }
+    __syncthreads();
+    mrfix::fft<1, M, NL, 1, LS, kNT>(sm, a.ax.tw);
+    float2 *dst = a.dst + (pbase * a.plane_rows + loc) * a.d_row;
+    const int64_t dstride = a.plane_rows * a.d_row;
+    for (int idx = threadIdx.x; idx < ncoils * L * a.n_out; idx += kNT) {
+        const int b = idx / a.n_out;
+        const int da = idx - b * a.n_out;
+        int q = da - a.shift_out;
+        if (q < 0) q += M;
+        dst[b * dstride + da] = c_scale(sm[b * LS + q], a.scale);
+    }
+}
+
+template <typename F>
+void set_attr(F *f, unsigned long long &mask) {
+    const int dev = mr_current_device();
+    if (!(mask & (1ull << dev))) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, mr_smem_limit());
+        mask |= 1ull << dev;
+    }
+}
+
+template <int DIR, int LM, int SM, int M, int XT>
+int launch_s3(const mr_strided_args &a, cudaStream_t s) {
+    static unsigned long long attr = 0;
+    set_attr(k_strided3<DIR, LM, SM, M, XT>, attr);
+    size_t smem = (size_t)M * XT * sizeof(float2);
+    if (SM == MR_SM_COILSUM) smem += (size_t)a.n_out * XT * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
+    if (nblk <= 0) return MR_SUCCESS;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+    k_strided3<DIR, LM, SM, M, XT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_strided3");
+    return MR_SUCCESS;
+}
+
+template <int M, int L, int NC, int KF>
+int launch_x3(const mr_x_args &a, cudaStream_t s) {
+    static unsigned long long attr = 0;
+    set_attr(k_xbd3<M, L, NC, KF>, attr);
+    const size_t smem = (size_t)NC * L * odd_stride<M>() * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nloc * a.nchunk;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
+    k_xbd3<M, L, NC, KF><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_xbd3");
+    return MR_SUCCESS;
+}
+
+}  // namespace
+
+// Instantiated strided configurations (length, tile width) and block-diagonal
+// configurations (length, rank, coils per tile). Every strided one is built in
+// the four modes the plans use.
+#define MR_S3_LIST(X) \
+    X(640, 32) X(640, 16) X(56, 256) X(56, 128) X(128, 64) X(128, 32) X(8, 256)
+#define MR_X3_LIST(X) X(640, 16, 2) X(128, 4, 4)
+
+int mr_fixed_strided_xt(int M, int smode) {
+    // the widest instantiated tile of this length for the store mode
+    int best = 0;
+#define MR_S3_PICK(m, xt)                                                            \
+    if (M == m) {                                                                    \
+        size_t b = (size_t)m * xt * sizeof(float2);                                  \
+        if (smode == MR_SM_COILSUM) b += (size_t)m * xt * sizeof(float2);            \
+        if (b <= (size_t)mr_smem_limit() && xt > best) best = xt;                    \
+    }
+    MR_S3_LIST(MR_S3_PICK)
+#undef MR_S3_PICK
+    return best;
+}
+
+int mr_launch_strided3(int dir, int lmode, int smode, const mr_strided_args &a, cudaStream_t s) {
+    const int M = a.ax.M, XT = a.xt;
+#define MR_S3_CASE(m, xt)                                                                     \
+    if (M == m && XT == xt) {                                                                 \
+        if (dir < 0 && lmode == MR_LM_BUF && smode == MR_SM_BUF) return launch_s3<-1, 0, 0, m, xt>(a, s); \
+        if (dir < 0 && lmode == MR_LM_XS && smode == MR_SM_BUF) return launch_s3<-1, 1, 0, m, xt>(a, s);  \
+        if (dir > 0 && lmode == MR_LM_BUF && smode == MR_SM_BUF) return launch_s3<1, 0, 0, m, xt>(a, s);  \
+        if (dir > 0 && lmode == MR_LM_BUF && smode == MR_SM_COILSUM) return launch_s3<1, 0, 1, m, xt>(a, s); \
+    }
+    MR_S3_LIST(MR_S3_CASE)
+#undef MR_S3_CASE
+    MR_FAIL(MR_ERR_INTERNAL, "no specialised strided pass for M = %d, tile %d", M, XT);
+}
+
+int mr_fixed_xbd_coils(int M, int L) {
+    int nc = 0;
+#define MR_X3_PICK(m, l, c) \
+    if (M == m && L == l) nc = c;
+    MR_X3_LIST(MR_X3_PICK)
+#undef MR_X3_PICK
+    return nc;
+}
+
+int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s) {
+    const int M = a.ax.M;
+#define MR_X3_CASE(m, l, c)                                                     \
+    if (M == m && a.L == l && a.nc == c) {                                      \
+        switch (a.K.kf) {                                                       \
+            case MR_KF_F32: return launch_x3<m, l, c, MR_KF_F32>(a, s);         \
+            case MR_KF_BF16: return launch_x3<m, l, c, MR_KF_BF16>(a, s);       \
+            default: return launch_x3<m, l, c, MR_KF_I16>(a, s);                \
+        }                                                                       \
+    }
+    MR_X3_LIST(MR_X3_CASE)
+#undef MR_X3_CASE
+    MR_FAIL(MR_ERR_INTERNAL, "no specialised block-diagonal pass for M = %d, L = %d", M, a.L);
+}
