@@ -65,6 +65,23 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """Largest value of x over the ranks (x itself without a process group)."""
+    if dist is None:
+        return float(x)
+    import torch
+
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(steps: int, world: int, ms_max: float) -> float:
+    """Whole-job applies/s of `world` independent replicas that each ran
+    `steps` applies, timed by the slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 def workload_config(name: str, wl: dict) -> dict:
     return {"workload": name, "traj_type": wl["traj_type"], "n_dim": list(wl["n_dim"]),
             "phi2_dim": list(wl["phi2_dim"]), "L": wl["L"], "n_coils": wl["n_coils"],
@@ -271,12 +288,8 @@ def run_ours(args):
     clocks = sampler.stop()
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms = float(ms_t.item())
-    value = world * args.steps / (ms / 1e3)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    value = replica_throughput(args.steps, world, ms)
 
     # ---- end-to-end through op(x) with host buffers ----
     y_h = torch.empty(x_h.shape, dtype=x_h.dtype).pin_memory()
@@ -295,12 +308,8 @@ def run_ours(args):
         y_h.copy_(out, non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    ms_e = e0.elapsed_time(e1)
-    me = torch.tensor([ms_e], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(me, op=dist.ReduceOp.MAX)
-    ms_e = float(me.item())
-    e2e = {"value": world * args.steps / (ms_e / 1e3), "unit": UNIT,
+    ms_e = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e = {"value": replica_throughput(args.steps, world, ms_e), "unit": UNIT,
            "h2d_bytes_per_step": int(x_h.numel() * 8), "d2h_bytes_per_step": int(y_h.numel() * 8)}
 
     # ---- roofline of the dominant kernel ----

@@ -112,10 +112,19 @@ def _ptr(array, name: str, dtype: str, allow_none: bool = False):
 def _size(array) -> int:
     if _is_torch(array):
         return int(array.numel())
+    cai = getattr(array, "__cuda_array_interface__", None)
+    if cai is None:
+        return int(getattr(array, "size", 0))
     n = 1
-    for s in array.__cuda_array_interface__["shape"]:
+    for s in cai["shape"]:
         n *= int(s)
     return n
+
+
+def _shape(array) -> tuple:
+    if _is_torch(array):
+        return tuple(array.shape)
+    return tuple(array.__cuda_array_interface__["shape"])
 
 
 def _check_size(array, expected: int, name: str) -> None:
@@ -304,16 +313,16 @@ def aha_toeplitz(cfg: MRConfig, x, SEs, phi2_toep, mask=None, out=None):
     _check_size(phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "phi2_toep")
     if cfg.is_masked and mask is None:
         raise ValueError("cfg.is_masked is set, so a mask is required")
+    px = _ptr(x, "x", "complex64")
+    ps = _ptr(SEs, "SEs", "complex64")
+    pk = _ptr(phi2_toep, "phi2_toep", "complex64")
+    pm = _ptr(mask, "mask", "int64", allow_none=True)
     if out is None:
-        out = _empty(tuple(x.shape) if _is_torch(x) else x.__cuda_array_interface__["shape"],
-                     "complex64", _device_of(x))
+        out = _empty(_shape(x), "complex64", _device_of(x))
     else:
         _check_size(out, _size(x), "out")
-    check(lib.mr_aha_toeplitz(ctypes.byref(cfg), _ptr(x, "x", "complex64"),
-                              _ptr(SEs, "SEs", "complex64"),
-                              _ptr(phi2_toep, "phi2_toep", "complex64"),
-                              _ptr(mask, "mask", "int64", allow_none=True),
-                              _ptr(out, "out", "complex64")), "mr_aha_toeplitz")
+    check(lib.mr_aha_toeplitz(ctypes.byref(cfg), px, ps, pk, pm, _ptr(out, "out", "complex64")),
+          "mr_aha_toeplitz")
     return out
 
 
@@ -479,13 +488,13 @@ class AhAOp:
         """``A^H A x`` (``mr_op_execute``), ordered on ``cfg.stream``."""
         self._check_open()
         _check_size(x, int(lib.mr_x_size(ctypes.byref(self._cfg))), "x")
+        px = _ptr(x, "x", "complex64")
         if out is not None:
             _check_size(out, _size(x), "out")
         else:
-            out = _empty(tuple(x.shape) if _is_torch(x) else x.__cuda_array_interface__["shape"],
-                         "complex64", _device_of(x))
-        check(lib.mr_op_execute(self._handle, _ptr(x, "x", "complex64"),
-                                _ptr(out, "out", "complex64")), "mr_op_execute")
+            out = _empty(_shape(x), "complex64", _device_of(x))
+        check(lib.mr_op_execute(self._handle, px, _ptr(out, "out", "complex64")),
+              "mr_op_execute")
         return out
 
     __call__ = apply
