@@ -16,6 +16,7 @@ from __future__ import annotations
 import argparse
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -42,13 +43,26 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libmr_aha_c.so")
 
 
-def _headers():
-    return list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list((ROOT / "include").rglob("*.h"))
+_INCLUDE = re.compile(r'^\s*#\s*include\s*"([^"]+)"', re.M)
+
+
+def _deps(src: Path, seen=None) -> set:
+    """Files `src` includes with quotes, recursively (csrc/ and include/)."""
+    seen = set() if seen is None else seen
+    for name in _INCLUDE.findall(src.read_text()):
+        for base in (src.parent, CSRC, ROOT / "include"):
+            f = (base / name).resolve()
+            if f.exists():
+                if f not in seen:
+                    seen.add(f)
+                    _deps(f, seen)
+                break
+    return seen
 
 
 def _compile(src: Path, force: bool, ptxas_v: bool) -> Path:
     obj = OBJ / (src.stem + ".o")
-    newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _deps(src)])
     if not force and obj.exists() and obj.stat().st_mtime >= newest:
         return obj
     cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-I", str(CSRC),

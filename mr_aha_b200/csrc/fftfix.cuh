@@ -127,3 +127,120 @@ __device__ __forceinline__ void fft(float2 *buf, const float2 *tw) {
 }
 
 }  // namespace mrfix
+
+namespace mrfix {
+
+// First pass reading its inputs through load(b, e) (element e of line b)
+// instead of shared memory: no barrier before it, outputs to shared memory.
+template <int R, int DIR, int M, int NL, int ES, int LS, int NT, int UA, class LoadF>
+__device__ __forceinline__ void pass_first(float2 *buf, float2 (&u)[UA], const LoadF &load) {
+    constexpr int MR = M / R;
+    constexpr int TOTAL = NL * MR;
+    constexpr int NB = (TOTAL + NT - 1) / NT;
+    constexpr bool EXACT = (TOTAL % NT) == 0;
+    static_assert(NB * R <= UA, "register stage too small");
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int w = tid + k * NT;
+        if (EXACT || w < TOTAL) {
+            const int i = w / NL;
+            const int b = w - i * NL;
+#pragma unroll
+            for (int t = 0; t < R; ++t) u[k * R + t] = load(b, i + t * MR);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int w = tid + k * NT;
+        if (EXACT || w < TOTAL) {
+            const int i = w / NL;
+            const int b = w - i * NL;
+            dft_small<R, DIR>(&u[k * R]);
+            float2 *d = buf + b * LS + (i * R) * ES;   // p = 1
+#pragma unroll
+            for (int t = 0; t < R; ++t) d[t * ES] = u[k * R + t];
+        }
+    }
+    __syncthreads();
+}
+
+// Last pass writing its outputs through store(b, e, v) instead of shared
+// memory (no barrier needed after its reads: shared memory is not written).
+template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int UA, class StoreF>
+__device__ __forceinline__ void pass_last(const float2 *buf, const float2 *__restrict__ tw,
+                                          float2 (&u)[UA], const StoreF &store) {
+    constexpr int MR = M / R;
+    constexpr int TOTAL = NL * MR;
+    constexpr int NB = (TOTAL + NT - 1) / NT;
+    constexpr int TSTEP = M / (P * R);
+    constexpr bool EXACT = (TOTAL % NT) == 0;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < NB; ++k) {
+        const int w = tid + k * NT;
+        if (EXACT || w < TOTAL) {
+            const int i = w / NL;
+            const int b = w - i * NL;
+            const float2 *s = buf + b * LS + i * ES;
+#pragma unroll
+            for (int t = 0; t < R; ++t) u[k * R + t] = s[t * MR * ES];
+            const int kk = i % P;
+            const int q = i / P;
+            if constexpr (P > 1) {
+                const int e1 = kk * TSTEP;
+#pragma unroll
+                for (int t = 1; t < R; ++t)
+                    u[k * R + t] = c_mul(u[k * R + t], tw_get<DIR>(tw, t * e1));
+            }
+            dft_small<R, DIR>(&u[k * R]);
+#pragma unroll
+            for (int t = 0; t < R; ++t) store(b, q * P * R + kk + t * P, u[k * R + t]);
+        }
+    }
+}
+
+template <bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, int S, int P, int UA,
+          class StoreF>
+__device__ __forceinline__ void run_io(float2 *buf, const float2 *tw, float2 (&u)[UA],
+                                       const StoreF &store) {
+    constexpr radix_list l = factor(M);
+    if constexpr (S < l.n) {
+        constexpr int R = l.r[S];
+        if constexpr (LASTG && S + 1 == l.n) {
+            pass_last<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u, store);
+        } else {
+            pass<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u);
+            run_io<LASTG, DIR, M, NL, ES, LS, NT, S + 1, P * R>(buf, tw, u, store);
+        }
+    }
+}
+
+struct no_store {
+    __device__ void operator()(int, int, float2) const {}
+};
+
+// Transform of NL lines. FIRSTG: the first pass reads load(b, e) (element e
+// of line b) instead of shared memory. LASTG: the last pass writes
+// store(b, e, v) instead of shared memory (the result is then not in buf;
+// the caller synchronises before reusing buf). Otherwise the result is in
+// buf in natural order.
+template <bool FIRSTG, bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, class LoadF,
+          class StoreF>
+__device__ __forceinline__ void fft_io(float2 *buf, const float2 *tw, const LoadF &load,
+                                       const StoreF &store) {
+    constexpr radix_list l = factor(M);
+    static_assert(l.n >= 1, "length not specialised");
+    static_assert(!(FIRSTG && LASTG) || l.n >= 2, "one-pass transform cannot do both");
+    constexpr int UA = max_stage(M, NL, NT);
+    float2 u[UA];
+    if constexpr (FIRSTG) {
+        constexpr int R0 = l.r[0];
+        pass_first<R0, DIR, M, NL, ES, LS, NT>(buf, u, load);
+        run_io<LASTG, DIR, M, NL, ES, LS, NT, 1, R0>(buf, tw, u, store);
+    } else {
+        run_io<LASTG, DIR, M, NL, ES, LS, NT, 0, 1>(buf, tw, u, store);
+    }
+}
+
+}  // namespace mrfix

@@ -34,6 +34,41 @@ __global__ void __launch_bounds__(kNT) k_strided3(const __grid_constant__ mr_str
             xp = a.xs_x + (int64_t)(sp % a.L) * a.img_plane + off0;
             sp_s = a.xs_s + (int64_t)(a.coil0 + sp / a.L) * a.img_plane + off0;
         }
+        if constexpr (mrfix::factor(M).n >= 2) {
+            // first pass reads global memory, last pass writes it: the tile
+            // is x-major, so consecutive threads touch consecutive x
+            auto load = [&](int b, int e) -> float2 {
+                int sa = e + a.shift_in;
+                if (sa >= M) sa -= M;
+                float2 v = make_float2(0.f, 0.f);
+                if (b < nx && sa < a.n_in) {
+                    const int64_t o = (int64_t)sa * a.s_axis + b;
+                    if constexpr (LM == MR_LM_BUF) v = srcp[o];
+                    else v = c_mul(__ldg(sp_s + o), __ldg(xp + o));
+                }
+                return v;
+            };
+            auto store = [&](int b, int q, float2 v) {
+                int da = q + a.shift_out;
+                if (da >= M) da -= M;
+                if (da < a.n_out && b < nx) {
+                    if constexpr (SM == MR_SM_BUF) {
+                        a.dst[(int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + b] =
+                            c_scale(v, a.scale);
+                    } else {
+                        const float2 w = c_mulc(
+                            __ldg(a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0 +
+                                  (int64_t)da * a.d_axis + b),
+                            v);
+                        const int ai = da * XT + b;
+                        acc[ai] = (cc == 0) ? w : c_add(acc[ai], w);
+                    }
+                }
+            };
+            mrfix::fft_io<true, true, DIR, M, XT, XT, 1, kNT>(sm, a.ax.tw, load, store);
+            __syncthreads();
+            continue;
+        }
 #pragma unroll 4
         for (int idx = threadIdx.x; idx < TILE; idx += kNT) {
             const int j = idx / XT;
