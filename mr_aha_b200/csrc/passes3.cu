@@ -8,10 +8,12 @@
 
 namespace {
 
-constexpr int kNT = 512;
+// Block sizes: 512 threads for tiles of more than 10240 elements (one CTA per
+// SM), 256 threads for smaller tiles, with registers capped so that two
+// independent CTAs share an SM (one loads or stores while the other computes).
 
-template <int DIR, int LM, int SM, int M, int XT>
-__global__ void __launch_bounds__(kNT) k_strided3(const __grid_constant__ mr_strided_args a) {
+template <int DIR, int LM, int SM, int M, int XT, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_strided3(const __grid_constant__ mr_strided_args a) {
     extern __shared__ float2 sm[];
     constexpr int TILE = M * XT;
     float2 *acc = sm + TILE;
@@ -125,8 +127,8 @@ constexpr int odd_stride() {
     return (M % 2 == 0) ? M + 1 : M + 2;
 }
 
-template <int M, int L, int NC, int KF>
-__global__ void __launch_bounds__(kNT) k_xbd3(const __grid_constant__ mr_x_args a) {
+template <int M, int L, int NC, int KF, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__ mr_x_args a) {
     extern __shared__ float2 sm[];
     constexpr int LS = odd_stride<M>();
     constexpr int NL = NC * L;
@@ -206,26 +208,28 @@ void set_attr(F *f, unsigned long long &mask) {
 
 template <int DIR, int LM, int SM, int M, int XT>
 int launch_s3(const mr_strided_args &a, cudaStream_t s) {
+    constexpr int kNT = (M * XT > 10240) ? 512 : 256;
     static unsigned long long attr = 0;
-    set_attr(k_strided3<DIR, LM, SM, M, XT>, attr);
+    set_attr(k_strided3<DIR, LM, SM, M, XT, kNT>, attr);
     size_t smem = (size_t)M * XT * sizeof(float2);
     if (SM == MR_SM_COILSUM) smem += (size_t)a.n_out * XT * sizeof(float2);
     const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
     if (nblk <= 0) return MR_SUCCESS;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
-    k_strided3<DIR, LM, SM, M, XT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    k_strided3<DIR, LM, SM, M, XT, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
     MR_LAUNCH_CHECK("k_strided3");
     return MR_SUCCESS;
 }
 
 template <int M, int L, int NC, int KF>
 int launch_x3(const mr_x_args &a, cudaStream_t s) {
+    constexpr int kNT = (NC * L * M > 10240) ? 512 : 256;
     static unsigned long long attr = 0;
-    set_attr(k_xbd3<M, L, NC, KF>, attr);
+    set_attr(k_xbd3<M, L, NC, KF, kNT>, attr);
     const size_t smem = (size_t)NC * L * odd_stride<M>() * sizeof(float2);
     const int64_t nblk = (int64_t)a.nloc * a.nchunk;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
-    k_xbd3<M, L, NC, KF><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    k_xbd3<M, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
     MR_LAUNCH_CHECK("k_xbd3");
     return MR_SUCCESS;
 }
@@ -236,20 +240,31 @@ int launch_x3(const mr_x_args &a, cudaStream_t s) {
 // configurations (length, rank, coils per tile). Every strided one is built in
 // the four modes the plans use.
 #define MR_S3_LIST(X) \
-    X(640, 32) X(640, 16) X(56, 256) X(56, 128) X(128, 64) X(128, 32) X(8, 256)
-#define MR_X3_LIST(X) X(640, 16, 2) X(128, 4, 4)
+    X(640, 32) X(640, 16) X(640, 8) X(56, 256) X(56, 128) X(128, 64) X(128, 32) X(8, 256)
+#define MR_X3_LIST(X) X(640, 16, 2) X(640, 16, 1) X(128, 4, 4)
+
+namespace {
+// Shared memory a tile may take: half the per-block limit (two CTAs per SM)
+// unless MR_AHA_B200_FULL_TILES is set.
+size_t tile_budget(bool half) { return (size_t)mr_smem_limit() / (half ? 2 : 1); }
+bool half_tiles() { return mr_env_int("MR_AHA_B200_FULL_TILES", 0) == 0; }
+}  // namespace
 
 int mr_fixed_strided_xt(int M, int smode) {
-    // the widest instantiated tile of this length for the store mode
+    // the widest instantiated tile of this length for the store mode within
+    // the tile budget; the full limit when no tile fits half of it
     int best = 0;
-#define MR_S3_PICK(m, xt)                                                            \
-    if (M == m) {                                                                    \
-        size_t b = (size_t)m * xt * sizeof(float2);                                  \
-        if (smode == MR_SM_COILSUM) b += (size_t)m * xt * sizeof(float2);            \
-        if (b <= (size_t)mr_smem_limit() && xt > best) best = xt;                    \
-    }
-    MR_S3_LIST(MR_S3_PICK)
+    for (int pass = 0; pass < 2 && best == 0; ++pass) {
+        const size_t budget = tile_budget(pass == 0 && half_tiles());
+#define MR_S3_PICK(m, xt)                                                 \
+        if (M == m) {                                                     \
+            size_t b = (size_t)m * xt * sizeof(float2);                   \
+            if (smode == MR_SM_COILSUM) b += (size_t)m * xt * sizeof(float2); \
+            if (b <= budget && xt > best) best = xt;                      \
+        }
+        MR_S3_LIST(MR_S3_PICK)
 #undef MR_S3_PICK
+    }
     return best;
 }
 
@@ -268,11 +283,17 @@ int mr_launch_strided3(int dir, int lmode, int smode, const mr_strided_args &a, 
 }
 
 int mr_fixed_xbd_coils(int M, int L) {
+    // the most coils per tile within the tile budget (as above)
     int nc = 0;
-#define MR_X3_PICK(m, l, c) \
-    if (M == m && L == l) nc = c;
-    MR_X3_LIST(MR_X3_PICK)
+    for (int pass = 0; pass < 2 && nc == 0; ++pass) {
+        const size_t budget = tile_budget(pass == 0 && half_tiles());
+#define MR_X3_PICK(m, l, c)                                                         \
+        if (M == m && L == l && (size_t)c * l * odd_stride<m>() * sizeof(float2) <= budget && \
+            c > nc)                                                                 \
+            nc = c;
+        MR_X3_LIST(MR_X3_PICK)
 #undef MR_X3_PICK
+    }
     return nc;
 }
 
