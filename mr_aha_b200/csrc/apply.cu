@@ -48,6 +48,7 @@ struct mr_aha_plan_s {
     // compile-time-specialised kernels (passes3.cu): tile widths, 0 if none
     int xt3_z_buf, xt3_z_cs, xt3_y_buf, xt3_y_cs;
     int nc3;
+    int nch;         // coils per tile of the half-length pass 3, 0 if none
     int launches;    // kernels per execute (accounting)
 };
 
@@ -68,13 +69,20 @@ static void plan_pick_v2(mr_aha_plan p, size_t lim) {
     }
     if (p->ax[0].small && p->fused) p->nc2 = mr_xbd2_coils(g.m[0], g.L, p->cfg.n_coils, lim);
     p->xt3_z_buf = p->xt3_z_cs = p->xt3_y_buf = p->xt3_y_cs = 0;
-    p->nc3 = 0;
+    p->nc3 = p->nch = 0;
     if (mr_env_int("MR_AHA_B200_NO_FIXED", 0)) return;
-    p->xt3_z_buf = mr_fixed_strided_xt(g.m[2], MR_SM_BUF);
-    p->xt3_z_cs = mr_fixed_strided_xt(g.m[2], MR_SM_COILSUM);
-    p->xt3_y_buf = mr_fixed_strided_xt(g.m[1], MR_SM_BUF);
-    p->xt3_y_cs = mr_fixed_strided_xt(g.m[1], MR_SM_COILSUM);
+    // tile widths may be forced per axis (tuning): MR_AHA_B200_XT_Z, _XT_Y.
+    // The first pass (image x coil maps, short z lines) runs fastest with
+    // narrow tiles: 32 columns of 56-point lines measured 5.2 ms against
+    // 9.4 ms for 256 columns at 320 x 320 x 56, L = 16, 12 coils.
+    const int wz = mr_env_int("MR_AHA_B200_XT_Z", 0), wy = mr_env_int("MR_AHA_B200_XT_Y", 0);
+    p->xt3_z_buf = mr_fixed_strided_xt(g.m[2], MR_SM_BUF, wz ? wz : (g.m[2] <= 64 ? 32 : 0));
+    p->xt3_z_cs = mr_fixed_strided_xt(g.m[2], MR_SM_COILSUM, wz);
+    p->xt3_y_buf = mr_fixed_strided_xt(g.m[1], MR_SM_BUF, wy);
+    p->xt3_y_cs = mr_fixed_strided_xt(g.m[1], MR_SM_COILSUM, wy);
     if (p->fused) p->nc3 = mr_fixed_xbd_coils(g.m[0], g.L);
+    // pass 3 pads x by cn[0] and crops the same window
+    if (p->fused) p->nch = mr_fixed_xbdh_coils(g.m[0], g.n[0], g.L);
 }
 
 // ---------------------------------------------------------------------------
@@ -487,7 +495,11 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.cmy = g.cm[1];
                 a.cmz = g.cm[2];
                 a.K = K;
-                if (p->nc3 > 0) {
+                if (p->nch > 0) {
+                    a.nc = p->nch;
+                    a.nchunk = (int)mr_cdiv(G, a.nc);
+                    rc = mr_launch_xbdh(a, s);
+                } else if (p->nc3 > 0) {
                     a.nc = p->nc3;
                     a.nchunk = (int)mr_cdiv(G, a.nc);
                     rc = mr_launch_xbd3(a, s);

@@ -77,13 +77,18 @@ int mr_launch_strided2(int dir, int lmode, int smode, const mr_strided_args &a, 
                        cudaStream_t s);
 int mr_launch_xbd2(const mr_x_args &a, cudaStream_t s);
 int mr_strided2_xts(int M, int n_out, int smode, int nfast, size_t limit);
-// Compile-time-specialised variants (passes3.cu): widest instantiated tile for
-// a length and store mode (0 if none), coils per tile of the instantiated
-// block-diagonal pass for (M, L) (0 if none).
-int mr_fixed_strided_xt(int M, int smode);
+// Compile-time-specialised variants (passes3.cu): tile width for a length and
+// store mode (`want` if instantiated, else the widest that fits; 0 if none),
+// coils per tile of the instantiated block-diagonal pass for (M, L) (0 if none).
+int mr_fixed_strided_xt(int M, int smode, int want = 0);
 int mr_launch_strided3(int dir, int lmode, int smode, const mr_strided_args &a, cudaStream_t s);
 int mr_fixed_xbd_coils(int M, int L);
 int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s);
+// Half-length pass 3 (passes3.cu) for M = 2 n_in with the crop window equal
+// to the pad window: coils per tile (0 if M != 2 n_in or not instantiated),
+// and its launcher (a.nc set to that).
+int mr_fixed_xbdh_coils(int M, int n_in, int L);
+int mr_launch_xbdh(const mr_x_args &a, cudaStream_t s);
 int mr_xbd2_coils(int M, int L, int ncoil, size_t limit);
 int mr_xbd2_stride(int M);
 int mr_launch_xplain(int dir, const mr_x_args &a, cudaStream_t s);

@@ -62,12 +62,12 @@ constexpr int max_stage(int M, int NL, int NT) {
     return m;
 }
 
-template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int UA>
+template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int TWS, int UA>
 __device__ __forceinline__ void pass(float2 *buf, const float2 *__restrict__ tw, float2 (&u)[UA]) {
     constexpr int MR = M / R;
     constexpr int TOTAL = NL * MR;
     constexpr int NB = (TOTAL + NT - 1) / NT;
-    constexpr int TSTEP = M / (P * R);
+    constexpr int TSTEP = TWS * (M / (P * R));
     constexpr bool EXACT = (TOTAL % NT) == 0;
     static_assert(NB * R <= UA, "register stage too small");
     const int tid = threadIdx.x;
@@ -106,24 +106,26 @@ __device__ __forceinline__ void pass(float2 *buf, const float2 *__restrict__ tw,
     __syncthreads();
 }
 
-template <int DIR, int M, int NL, int ES, int LS, int NT, int S, int P, int UA>
+template <int DIR, int M, int NL, int ES, int LS, int NT, int TWS, int S, int P, int UA>
 __device__ __forceinline__ void run(float2 *buf, const float2 *tw, float2 (&u)[UA]) {
     constexpr radix_list l = factor(M);
     if constexpr (S < l.n) {
         constexpr int R = l.r[S];
-        pass<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u);
-        run<DIR, M, NL, ES, LS, NT, S + 1, P * R>(buf, tw, u);
+        pass<R, DIR, M, P, NL, ES, LS, NT, TWS>(buf, tw, u);
+        run<DIR, M, NL, ES, LS, NT, TWS, S + 1, P * R>(buf, tw, u);
     }
 }
 
 // In-place transform of NL lines of length M held in shared memory (element
-// e of line b at buf[b * LS + e * ES]) by NT threads.
-template <int DIR, int M, int NL, int ES, int LS, int NT>
+// e of line b at buf[b * LS + e * ES]) by NT threads. The twiddle table holds
+// W_{TWS M}^e: TWS = 1 for a table of this length, 2 for the table of the
+// doubled length (a length-M transform inside a length-2M one).
+template <int DIR, int M, int NL, int ES, int LS, int NT, int TWS = 1>
 __device__ __forceinline__ void fft(float2 *buf, const float2 *tw) {
     static_assert(factor(M).n > 0, "length not specialised");
     constexpr int UA = max_stage(M, NL, NT);
     float2 u[UA];
-    run<DIR, M, NL, ES, LS, NT, 0, 1>(buf, tw, u);
+    run<DIR, M, NL, ES, LS, NT, TWS, 0, 1>(buf, tw, u);
 }
 
 }  // namespace mrfix
@@ -210,7 +212,7 @@ __device__ __forceinline__ void run_io(float2 *buf, const float2 *tw, float2 (&u
         if constexpr (LASTG && S + 1 == l.n) {
             pass_last<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u, store);
         } else {
-            pass<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u);
+            pass<R, DIR, M, P, NL, ES, LS, NT, 1>(buf, tw, u);
             run_io<LASTG, DIR, M, NL, ES, LS, NT, S + 1, P * R>(buf, tw, u, store);
         }
     }

@@ -197,6 +197,95 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__
     }
 }
 
+// Pass 3 when the transform length is M = 2N, the row holds N samples (zero
+// padding to M) and the output is cropped to the same window. The pad and
+// crop phase ramps then cancel (the block multiply is diagonal in k), and
+// with t[n] = W_M^n (W_M = exp(-2 pi i / M)):
+//   X[2m] = FFT_N(x)[m],  X[2m+1] = FFT_N(x t)[m],
+//   y[n]  = IFFT_N(Z_even)[n] + conj(t[n]) IFFT_N(Z_odd)[n],
+// four length-N transforms of N-sample lines in place of two length-M
+// transforms of half-empty ones. Row b = (coil, rank) of the tile keeps its
+// even half-spectrum in line 2b and its odd one in line 2b + 1.
+template <int N, int L, int NC, int KF, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__ mr_x_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int LS = odd_stride<N>();
+    constexpr int NR = NC * L;
+    constexpr int NL = 2 * NR;
+    const int chunk = (int)(blockIdx.x % a.nchunk);
+    const int loc = (int)(blockIdx.x / a.nchunk);
+    const int jy = loc % a.My;
+    const int jz = loc / a.My;
+    const int c0 = chunk * NC;
+    const int ncoils = min(NC, a.ncoil - c0);
+    const int nrow = ncoils * L;
+    const int64_t pbase = (int64_t)c0 * L;
+    const float2 *tw = a.ax.tw;  // W_M^e, e < M
+    const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
+    const int64_t rstride = a.plane_rows * a.s_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < NR * N; idx += kNT) {
+        const int b = idx / N;
+        const int n = idx - b * N;
+        float2 v = make_float2(0.f, 0.f);
+        if (b < nrow) v = src[b * rstride + n];
+        sm[(2 * b) * LS + n] = v;
+        sm[(2 * b + 1) * LS + n] = c_mul(v, __ldg(tw + n));
+    }
+    __syncthreads();
+    mrfix::fft<-1, N, NL, 1, LS, kNT, 2>(sm, tw);
+    const int ky = mr_nat2cent_d(jy, a.My, a.cmy);
+    const int kz = mr_nat2cent_d(jz, a.Mz, a.cmz);
+    // a warp takes 16 consecutive m of one coil in both parities: lanes 0-15
+    // the even k = 2m, lanes 16-31 the odd k = 2m + 1 (each half-warp reads
+    // 16 consecutive words of one line)
+    constexpr int MB = (N + 15) / 16;
+    constexpr int ITEMS = NC * MB * 32;
+    for (int w = threadIdx.x; w < ITEMS; w += kNT) {
+        const int lane = w & 31;
+        const int wi = w >> 5;
+        const int k = wi / MB;
+        const int m = (wi - k * MB) * 16 + (lane & 15);
+        const int par = lane >> 4;
+        if (m >= N || k >= ncoils) continue;
+        const int jx = 2 * m + par;
+        float2 *line = sm + (2 * k * L + par) * LS + m;
+        float2 v[1][L], y[1][L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[0][l] = line[2 * l * LS];
+        bool zero = false;
+        int64_t row;
+        if (a.K.inv) {
+            const int r = __ldg(a.K.inv + jx + (int64_t)(2 * N) * (jy + (int64_t)a.My * jz));
+            zero = r < 0;
+            row = zero ? 0 : r;
+        } else {
+            row = mr_nat2cent_d(jx, 2 * N, a.cmx) + (int64_t)(2 * N) * (ky + (int64_t)a.My * kz);
+        }
+        if (zero) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
+        } else {
+            const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
+            bd_block<L, 1, KF>(v, y, kl, a.upper);
+        }
+#pragma unroll
+        for (int l = 0; l < L; ++l) line[2 * l * LS] = y[0][l];
+    }
+    __syncthreads();
+    mrfix::fft<1, N, NL, 1, LS, kNT, 2>(sm, tw);
+    float2 *dst = a.dst + (pbase * a.plane_rows + loc) * a.d_row;
+    const int64_t dstride = a.plane_rows * a.d_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < nrow * N; idx += kNT) {
+        const int b = idx / N;
+        const int n = idx - b * N;
+        const float2 e = sm[(2 * b) * LS + n];
+        const float2 o = sm[(2 * b + 1) * LS + n];
+        dst[b * dstride + n] = c_scale(c_add(e, c_mulc(__ldg(tw + n), o)), a.scale);
+    }
+}
+
 template <typename F>
 void set_attr(F *f, unsigned long long &mask) {
     const int dev = mr_current_device();
@@ -234,14 +323,30 @@ int launch_x3(const mr_x_args &a, cudaStream_t s) {
     return MR_SUCCESS;
 }
 
+template <int N, int L, int NC, int KF>
+int launch_xh(const mr_x_args &a, cudaStream_t s) {
+    constexpr int kNT = (NC * L * 2 * N > 10240) ? 512 : 256;
+    static unsigned long long attr = 0;
+    set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
+    const size_t smem = (size_t)2 * NC * L * odd_stride<N>() * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nloc * a.nchunk;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
+    k_xbdh<N, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_xbdh");
+    return MR_SUCCESS;
+}
+
 }  // namespace
 
 // Instantiated strided configurations (length, tile width) and block-diagonal
 // configurations (length, rank, coils per tile). Every strided one is built in
 // the four modes the plans use.
 #define MR_S3_LIST(X) \
-    X(640, 32) X(640, 16) X(640, 8) X(56, 256) X(56, 128) X(128, 64) X(128, 32) X(8, 256)
+    X(640, 32) X(640, 16) X(640, 8) X(56, 256) X(56, 128) X(56, 64) X(56, 32) X(56, 16) \
+    X(128, 64) X(128, 32) X(8, 256)
 #define MR_X3_LIST(X) X(640, 16, 2) X(640, 16, 1) X(128, 4, 4)
+// half-length block-diagonal configurations (N = M / 2, rank, coils per tile)
+#define MR_XH_LIST(X) X(320, 16, 1) X(64, 4, 4)
 
 namespace {
 // Shared memory a tile may take: half the per-block limit (two CTAs per SM)
@@ -250,10 +355,20 @@ size_t tile_budget(bool half) { return (size_t)mr_smem_limit() / (half ? 2 : 1);
 bool half_tiles() { return mr_env_int("MR_AHA_B200_FULL_TILES", 0) == 0; }
 }  // namespace
 
-int mr_fixed_strided_xt(int M, int smode) {
-    // the widest instantiated tile of this length for the store mode within
-    // the tile budget; the full limit when no tile fits half of it
+int mr_fixed_strided_xt(int M, int smode, int want) {
+    // `want` when it is instantiated and fits; else the widest instantiated
+    // tile of this length for the store mode within the tile budget, the
+    // full limit when no tile fits half of it
     int best = 0;
+    if (want > 0) {
+#define MR_S3_WANT(m, xt)                                                      \
+        if (M == m && want == xt &&                                            \
+            (size_t)m * xt * sizeof(float2) * (smode == MR_SM_COILSUM ? 2 : 1) <= \
+                (size_t)mr_smem_limit())                                       \
+            return xt;
+        MR_S3_LIST(MR_S3_WANT)
+#undef MR_S3_WANT
+    }
     for (int pass = 0; pass < 2 && best == 0; ++pass) {
         const size_t budget = tile_budget(pass == 0 && half_tiles());
 #define MR_S3_PICK(m, xt)                                                 \
@@ -310,4 +425,34 @@ int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s) {
     MR_X3_LIST(MR_X3_CASE)
 #undef MR_X3_CASE
     MR_FAIL(MR_ERR_INTERNAL, "no specialised block-diagonal pass for M = %d, L = %d", M, a.L);
+}
+
+int mr_fixed_xbdh_coils(int M, int n_in, int L) {
+    if (M != 2 * n_in || mr_env_int("MR_AHA_B200_NO_HALF", 0)) return 0;
+    const int N = n_in;
+    int nc = 0;
+#define MR_XH_PICK(n, l, c)                                                                  \
+    if (N == n && L == l && (size_t)2 * c * l * odd_stride<n>() * sizeof(float2) <=          \
+                                (size_t)mr_smem_limit() && c > nc)                           \
+        nc = c;
+    MR_XH_LIST(MR_XH_PICK)
+#undef MR_XH_PICK
+    return nc;
+}
+
+int mr_launch_xbdh(const mr_x_args &a, cudaStream_t s) {
+    const int N = a.n_in;
+    if (a.ax.M != 2 * N || a.n_out != N || a.shift_out != a.shift_in)
+        MR_FAIL(MR_ERR_INTERNAL, "half-length block-diagonal pass needs M = 2 N and equal windows");
+#define MR_XH_CASE(n, l, c)                                                   \
+    if (N == n && a.L == l && a.nc == c) {                                    \
+        switch (a.K.kf) {                                                     \
+            case MR_KF_F32: return launch_xh<n, l, c, MR_KF_F32>(a, s);       \
+            case MR_KF_BF16: return launch_xh<n, l, c, MR_KF_BF16>(a, s);     \
+            default: return launch_xh<n, l, c, MR_KF_I16>(a, s);              \
+        }                                                                     \
+    }
+    MR_XH_LIST(MR_XH_CASE)
+#undef MR_XH_CASE
+    MR_FAIL(MR_ERR_INTERNAL, "no half-length block-diagonal pass for N = %d, L = %d", N, a.L);
 }
