@@ -59,6 +59,41 @@ MR_EXPORT int mr_b200_aha_toeplitz_noalloc(const mr_config *cfg, const mr_comple
                                            const mr_complex *d_phi2_toep,
                                            const int64_t *d_mask, mr_complex *d_AhAx);
 
+/* ---- Conjugate gradients on the device (no reference counterpart: the
+ * reference's API stops at the operator and leaves the solver to the caller).
+ * Solves (A^H A + lambda I) x = b for an operator `op`, with b and x device
+ * arrays shaped like the operator's input ([Nx,Ny,Nz,L] complex64). Vectors
+ * are FP32; inner products are accumulated in FP64 in a fixed order, so
+ * results are deterministic; the step scalars stay in device memory, so no
+ * iteration waits for the host. Work: three more vectors of x's size. */
+typedef struct mr_b200_cg_s *mr_b200_cg;
+
+#define MR_B200_CG_ZERO_X 1 /* start from x = 0 (x's contents are ignored)      */
+#define MR_B200_CG_GRAPH 2  /* replay iterations from a captured CUDA graph     */
+
+/* Set up a solve: r = b - (A^H A + lambda) x, p = r. Keeps b and x borrowed
+ * (x is updated in place by every step). max_iters bounds the residual
+ * history. Asynchronous on the operator's stream. */
+MR_EXPORT int mr_b200_cg_create(mr_op op, const mr_complex *d_b, mr_complex *d_x, double lambda,
+                                int flags, int max_iters, mr_b200_cg *cg);
+
+/* Issue n_iter iterations (one apply and three vector kernels each) on the
+ * solver's own stream, ordered after earlier work on the operator's stream and
+ * before later work there. Returns without waiting for the GPU. */
+MR_EXPORT int mr_b200_cg_step(mr_b200_cg cg, int n_iter);
+
+/* Wait for the solver and copy |r_k|^2 for k = 0 .. min(iterations, max_iters)
+ * (at most `max` values) to host `rr`; *n receives how many exist. */
+MR_EXPORT int mr_b200_cg_residuals(mr_b200_cg cg, double *rr, int max, int *n);
+
+/* Wait for the solver and free it (b and x stay the caller's). */
+MR_EXPORT int mr_b200_cg_destroy(mr_b200_cg cg);
+
+/* create + n_iter steps + residuals (rr: n_iter + 1 values, may be NULL) +
+ * destroy. Synchronous. */
+MR_EXPORT int mr_b200_cg_solve(mr_op op, const mr_complex *d_b, mr_complex *d_x, int n_iter,
+                               double lambda, int flags, double *rr);
+
 #ifdef __cplusplus
 }
 #endif

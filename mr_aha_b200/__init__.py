@@ -13,6 +13,7 @@ from .api import (  # noqa: F401
     DEFAULT_MASK_RADIUS,
     AhAOp,
     AhAPlan,
+    CGSolver,
     aha_toeplitz,
     calc_mask,
     calc_toep,

@@ -540,6 +540,42 @@ class AhAOp:
         return [(raw[32 * k: 32 * k + 32].split(b"\0")[0].decode(), float(ms[k]))
                 for k in range(n.value)]
 
+    def cg(self, b, n_iter: int = 30, lam: float = 0.0, x0=None, out=None,
+           graph: bool = True):
+        """Solve ``(A^H A + lam I) x = b`` with ``n_iter`` conjugate-gradient
+        iterations on the device (``mr_b200_cg_solve``; no reference
+        counterpart). Starts from ``x0`` (copied into ``out``) or from zero.
+        Returns ``(x, rr)`` with ``rr[k] = |r_k|^2`` (numpy float64,
+        ``n_iter + 1`` values). Synchronous."""
+        self._check_open()
+        n = int(lib.mr_x_size(ctypes.byref(self._cfg)))
+        _check_size(b, n, "b")
+        pb = _ptr(b, "b", "complex64")
+        if out is None:
+            out = _empty(_shape(b), "complex64", _device_of(b))
+        else:
+            _check_size(out, n, "out")
+        flags = CG_GRAPH if graph else 0
+        if x0 is None:
+            flags |= CG_ZERO_X
+        else:
+            _check_size(x0, n, "x0")
+            out[...] = x0
+        rr = (ctypes.c_double * (n_iter + 1))()
+        check(lib.mr_b200_cg_solve(self._handle, pb, _ptr(out, "out", "complex64"), int(n_iter),
+                                   float(lam), flags, rr), "mr_b200_cg_solve")
+        import numpy as np
+
+        return out, np.array(rr[:], dtype=np.float64)
+
+    def cg_solver(self, b, x, lam: float = 0.0, max_iters: int = 1000, zero_x: bool = True,
+                  graph: bool = True) -> "CGSolver":
+        """A step-wise solver on this operator (``mr_b200_cg_create``): ``x``
+        is updated in place by ``step(n)``; ``b`` and ``x`` must stay alive
+        until ``close()``."""
+        self._check_open()
+        return CGSolver(self, b, x, lam, max_iters, zero_x, graph)
+
     @property
     def info(self) -> dict:
         self._check_open()
@@ -593,6 +629,66 @@ class AhAOp:
         try:
             self.close()
         except Exception:  # pragma: no cover
+            pass
+
+
+CG_ZERO_X = 1
+CG_GRAPH = 2
+
+
+class CGSolver:
+    """Conjugate gradients kept resident on the device (``mr_b200_cg_*``):
+    its vectors, step scalars and residual history stay in device memory
+    between ``step`` calls, which return without waiting for the GPU."""
+
+    def __init__(self, op: AhAOp, b, x, lam: float, max_iters: int, zero_x: bool, graph: bool):
+        n = int(lib.mr_x_size(ctypes.byref(op._cfg)))
+        _check_size(b, n, "b")
+        _check_size(x, n, "x")
+        self._op = op
+        self._keep = (b, x)
+        self.x = x
+        self.max_iters = int(max_iters)
+        self._handle = ctypes.c_void_p()
+        flags = (CG_ZERO_X if zero_x else 0) | (CG_GRAPH if graph else 0)
+        check(lib.mr_b200_cg_create(op._handle, _ptr(b, "b", "complex64"),
+                                    _ptr(x, "x", "complex64"), float(lam), flags,
+                                    self.max_iters, ctypes.byref(self._handle)),
+              "mr_b200_cg_create")
+
+    def step(self, n: int = 1) -> None:
+        if not self._handle:
+            raise RuntimeError("this CGSolver has already been closed")
+        check(lib.mr_b200_cg_step(self._handle, int(n)), "mr_b200_cg_step")
+
+    def residuals(self):
+        """``|r_k|^2`` for the iterations done so far (waits for the GPU)."""
+        import numpy as np
+
+        if not self._handle:
+            raise RuntimeError("this CGSolver has already been closed")
+        buf = (ctypes.c_double * (self.max_iters + 1))()
+        n = ctypes.c_int(0)
+        check(lib.mr_b200_cg_residuals(self._handle, buf, self.max_iters + 1, ctypes.byref(n)),
+              "mr_b200_cg_residuals")
+        return np.array(buf[: min(n.value, self.max_iters + 1)], dtype=np.float64)
+
+    def close(self) -> None:
+        if self._handle:
+            lib.mr_b200_cg_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+            self._keep = ()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
             pass
 
 

@@ -133,3 +133,9 @@ int mr_plan_launch_count(mr_aha_plan plan);
 size_t mr_plan_struct_size();
 int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, void *storage,
                              size_t *needed);
+
+// Operator internals shared with the solver (op.cu).
+int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s);
+const mr_config *mr_op_config(mr_op op);
+int mr_op_device(mr_op op);
+cudaStream_t mr_op_stream(mr_op op);

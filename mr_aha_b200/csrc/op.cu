@@ -244,6 +244,10 @@ int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s) {
     return mr_plan_execute_k(op->plan, x, op->S, op_kernel_ref(op), op->mask, out, s);
 }
 
+const mr_config *mr_op_config(mr_op op) { return &op->cfg; }
+int mr_op_device(mr_op op) { return op->dev; }
+cudaStream_t mr_op_stream(mr_op op) { return op->stream; }
+
 extern "C" int mr_op_execute(mr_op op, const mr_complex *d_x, mr_complex *d_AhAx) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr, "mr_op_execute: op is NULL");

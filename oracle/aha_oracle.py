@@ -409,3 +409,75 @@ def rel_l2(a, b) -> float:
     b = np.asarray(b, dtype=np.complex128)
     nb = float(np.linalg.norm(b))
     return float(np.linalg.norm(a - b)) / (nb if nb else 1.0)
+
+
+# --------------------------------------------------------------------------
+# Conjugate gradients (no reference counterpart: the reference stops at the
+# operator; this is the FP64 oracle of the device solver)
+# --------------------------------------------------------------------------
+
+def cg(apply, b: np.ndarray, n_iter: int, lam: float = 0.0, x0=None):
+    """FP64 conjugate gradients for ``(A^H A + lam I) x = b`` (Hestenes &
+    Stiefel 1952), step for step what the device solver computes:
+    ``q = apply(p) + lam p; alpha = |r|^2 / Re<p, q>`` (0 if not positive);
+    ``x += alpha p; r -= alpha q; beta = |r_new|^2 / |r|^2; p = r + beta p``.
+    ``apply`` maps a complex128 array to ``A^H A`` of it. Returns ``x`` and
+    ``|r_k|^2`` for ``k = 0 .. n_iter``."""
+    b = np.asarray(b, dtype=np.complex128)
+    if x0 is None:
+        x = np.zeros_like(b)
+        r = b.copy()
+    else:
+        x = np.array(x0, dtype=np.complex128)
+        r = b - apply(x) - lam * x
+    p = r.copy()
+    rr = float(np.vdot(r, r).real)
+    hist = [rr]
+    for _ in range(n_iter):
+        q = apply(p) + lam * p
+        pq = float(np.vdot(p, q).real)
+        alpha = rr / pq if pq > 0 else 0.0
+        x += alpha * p
+        r -= alpha * q
+        rr_new = float(np.vdot(r, r).real)
+        beta = rr_new / rr if rr > 0 else 0.0
+        rr = rr_new
+        hist.append(rr)
+        p = r + beta * p
+    return x, np.array(hist)
+
+
+def dequantized_kernel(K: np.ndarray, fmt: str) -> np.ndarray:
+    """The complex64 values a 16-bit-stored kernel represents (no reference
+    counterpart; the library's storage formats): per location q (last axes
+    flattened; axis 0 is the packed component t), ``m = max |re|, |im|``;
+    int16: ``scale = m / 32767``, ``code = rint(v / scale)`` (float32
+    arithmetic, ties to even, clamped to +-32767), value ``code * scale``;
+    bf16: ``scale = m``, value ``bf16(v / scale) * scale``. ``m = 0`` gives
+    scale 1. Used as the kernel of the FP64 oracle of a 16-bit operator."""
+    K = np.asarray(K, dtype=np.complex64)
+    shape = K.shape
+    K2 = K.reshape(shape[0], -1)
+    re = K2.real.astype(np.float32)
+    im = K2.imag.astype(np.float32)
+    m = np.maximum(np.abs(re), np.abs(im)).max(axis=0).astype(np.float32)
+    if fmt == "int16":
+        sc = np.where(m > 0, m / np.float32(32767.0), np.float32(1.0)).astype(np.float32)
+        inv = (np.float32(1.0) / sc).astype(np.float32)
+
+        def q(v):
+            c = np.clip((v * inv).astype(np.float32), -32767.0, 32767.0)
+            return (np.rint(c).astype(np.int16).astype(np.float32) * sc).astype(np.float32)
+    elif fmt == "bf16":
+        sc = np.where(m > 0, m, np.float32(1.0)).astype(np.float32)
+        inv = (np.float32(1.0) / sc).astype(np.float32)
+
+        def q(v):
+            u = (v * inv).astype(np.float32).view(np.uint32).astype(np.uint64)
+            # round to nearest even on the upper 16 bits (finite inputs)
+            u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+            return (u.astype(np.uint32).view(np.float32) * sc).astype(np.float32)
+    else:
+        raise ValueError(f"unknown 16-bit format {fmt!r}")
+    out = (q(re) + 1j * q(im)).astype(np.complex64)
+    return out.reshape(shape)

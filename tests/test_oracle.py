@@ -133,3 +133,53 @@ def test_oracle_catches_a_planted_error():
     bad = O.aha_toeplitz(p["traj_type"], p["n_dim"], p["phi2_dim"], p["L"], p["x"], p["SEs"], K,
                          blocks=np.conj(blocks))
     assert O.rel_l2(bad, good) > 1e-2
+
+
+def test_oracle_cg_solves_spd_system():
+    """The oracle CG reaches the direct solution of a small Hermitian positive
+    definite system in n iterations (finite termination), with and without a
+    start vector and a Tikhonov term."""
+    rng = np.random.default_rng(11)
+    n = 24
+    Q, _ = np.linalg.qr(synth.crandn(rng, (n, n), np.complex128))
+    A = (Q * np.linspace(1.0, 8.0, n)) @ Q.conj().T
+    b = synth.crandn(rng, (n,), np.complex128)
+    for lam, x0 in ((0.0, None), (0.5, synth.crandn(rng, (n,), np.complex128))):
+        x, rr = O.cg(lambda v: A @ v, b, n, lam=lam, x0=x0)
+        ref = np.linalg.solve(A + lam * np.eye(n), b)
+        assert O.rel_l2(x, ref) <= 1e-9
+        assert rr[-1] <= 1e-18 * rr[0]
+
+
+def test_oracle_cg_on_the_operator():
+    """CG on the oracle's own A^H A (a Gram-derived kernel, Hermitian PSD)
+    decreases the A^H A-norm error monotonically, as CG must."""
+    p = synth.reference_case(CASES[6])
+    K = O.calc_toep(p["traj_type"], p["phi2_dim"], p["L"], p["phi2"], p["traj"])
+
+    def A(v):
+        return O.aha_toeplitz(p["traj_type"], p["n_dim"], p["phi2_dim"], p["L"], v, p["SEs"], K)
+
+    b = A(p["x"].astype(np.complex128))
+    errs = []
+    for k in (2, 4, 8):
+        x, _ = O.cg(A, b, k)
+        e = x - p["x"]
+        errs.append(float(np.vdot(e, A(e)).real))
+    assert errs[0] > errs[1] > errs[2]
+
+
+def test_dequantized_kernel_formats():
+    """The 16-bit storage restatement: int16 codes within half a step of the
+    value, bf16 within 2^-9 relative of the location's largest component, and
+    exact round trips of representable values."""
+    rng = np.random.default_rng(4)
+    K = synth.crandn(rng, (10, 3, 5)).astype(np.complex64)
+    K[:, 0, 0] = 0
+    for fmt, tol in (("int16", 0.5 / 32767), ("bf16", 2.0 ** -8)):
+        Kq = O.dequantized_kernel(K, fmt)
+        m = np.maximum(np.abs(K.real), np.abs(K.imag)).max(axis=0)
+        d = np.maximum(np.abs((Kq - K).real), np.abs((Kq - K).imag))
+        assert np.all(d <= tol * m * 1.0001 + 1e-30)
+        assert np.array_equal(O.dequantized_kernel(Kq, fmt) if fmt == "bf16" else Kq, Kq)
+        assert np.all(Kq[:, 0, 0] == 0)
