@@ -40,6 +40,18 @@ MR_EXPORT int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 
+/* No reference counterpart (the reference fixes its cuFFT plans and kernel
+ * families at plan time). Autotune the operator: time full applies (`reps`
+ * each, on a constant trial input) for every candidate kernel of each pass
+ * -- strided-pass tile widths and kernel generation, pass-3 kernel (half
+ * length / specialised / in-place / ping-pong) and coils per tile -- one pass
+ * at a time, and keep the fastest. Later operators and plans of the same
+ * geometry in this process start from the tuned choice. Every candidate
+ * meets the same accuracy bar; results of different kernel generations differ
+ * only by FP32 rounding. *ms (may be NULL) receives the tuned apply time.
+ * Synchronous. */
+MR_EXPORT int mr_b200_op_autotune(mr_op op, int reps, float *ms);
+
 /* Size of the library's static device scratch array used by
  * mr_b200_aha_toeplitz_noalloc (reserved on every GPU that loads the
  * library, until the process exits). */
@@ -58,6 +70,31 @@ MR_EXPORT int mr_b200_aha_toeplitz_noalloc(const mr_config *cfg, const mr_comple
                                            const mr_complex *d_SEs,
                                            const mr_complex *d_phi2_toep,
                                            const int64_t *d_mask, mr_complex *d_AhAx);
+
+/* ---- Batched apply of independent operators (no reference counterpart:
+ * the reference applies one operator per call). The operators may differ in
+ * size, rank, coil count and trajectory type; all must live on one device and
+ * appear once. Their passes run on n_streams worker streams (largest
+ * operators first, each onto the least-loaded stream), so small operators
+ * overlap on the GPU with large ones. */
+typedef struct mr_b200_batch_s *mr_b200_batch;
+
+#define MR_B200_BATCH_GRAPH 1 /* capture the batch as one CUDA graph; replay it
+                                 (captured again when the array pointers change) */
+#define MR_B200_BATCH_TUNE 2  /* mr_b200_op_autotune each distinct geometry at
+                                 creation (synchronous) */
+
+MR_EXPORT int mr_b200_batch_create(const mr_op *ops, int n_ops, int n_streams, int flags,
+                                   mr_b200_batch *batch);
+
+/* out[i] = A_i^H A_i x[i] for every operator i, ordered after earlier work on
+ * `stream` (a cudaStream_t; NULL = legacy default) and before later work
+ * there. Returns without waiting. Operators must not be executed elsewhere
+ * while a batch execution is in flight (their work buffers are in use). */
+MR_EXPORT int mr_b200_batch_execute(mr_b200_batch batch, const mr_complex *const *d_x,
+                                    mr_complex *const *d_out, void *stream);
+
+MR_EXPORT int mr_b200_batch_destroy(mr_b200_batch batch);
 
 /* ---- Conjugate gradients on the device (no reference counterpart: the
  * reference's API stops at the operator and leaves the solver to the caller).

@@ -13,6 +13,7 @@ from .api import (  # noqa: F401
     DEFAULT_MASK_RADIUS,
     AhAOp,
     AhAPlan,
+    Batch,
     CGSolver,
     aha_toeplitz,
     calc_mask,

@@ -190,6 +190,11 @@ PROTOTYPES = {
     "mr_b200_op_profile": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_float),
                                           ctypes.c_char_p, ctypes.c_int,
                                           ctypes.POINTER(ctypes.c_int)]),
+    "mr_b200_op_autotune": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    "mr_b200_batch_create": (ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.POINTER(_P)]),
+    "mr_b200_batch_execute": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
+    "mr_b200_batch_destroy": (ctypes.c_int, [_P]),
     "mr_b200_cg_create": (ctypes.c_int, [_P, _P, _P, ctypes.c_double, ctypes.c_int,
                                          ctypes.c_int, ctypes.POINTER(_P)]),
     "mr_b200_cg_step": (ctypes.c_int, [_P, ctypes.c_int]),

@@ -516,6 +516,15 @@ class AhAOp:
               "mr_b200_op_kernel_format")
         return {v: k for k, v in KERNEL_FORMATS.items()}[f.value]
 
+    def autotune(self, reps: int = 2) -> float:
+        """Pick the fastest kernel of every pass by timing full applies
+        (``mr_b200_op_autotune``); returns the tuned apply time in ms."""
+        self._check_open()
+        ms = ctypes.c_float(0.0)
+        check(lib.mr_b200_op_autotune(self._handle, int(reps), ctypes.byref(ms)),
+              "mr_b200_op_autotune")
+        return float(ms.value)
+
     @property
     def launches_per_apply(self) -> int:
         self._check_open()
@@ -634,6 +643,64 @@ class AhAOp:
 
 CG_ZERO_X = 1
 CG_GRAPH = 2
+BATCH_GRAPH = 1
+BATCH_TUNE = 2
+
+
+class Batch:
+    """Apply many independent operators together (``mr_b200_batch_*``; no
+    reference counterpart): ``batch(xs)`` returns ``[A_i^H A_i xs[i]]``.
+    ``graph=True`` replays one captured CUDA graph per set of array
+    pointers; ``tune=True`` autotunes each distinct geometry first."""
+
+    def __init__(self, ops, n_streams: int = 4, graph: bool = True, tune: bool = False):
+        self._ops = list(ops)
+        if not self._ops:
+            raise ValueError("a batch needs at least one operator")
+        for o in self._ops:
+            o._check_open()
+        arr = (ctypes.c_void_p * len(self._ops))(*[o._handle.value for o in self._ops])
+        self._handle = ctypes.c_void_p()
+        flags = (BATCH_GRAPH if graph else 0) | (BATCH_TUNE if tune else 0)
+        check(lib.mr_b200_batch_create(arr, len(self._ops), int(n_streams), flags,
+                                       ctypes.byref(self._handle)), "mr_b200_batch_create")
+
+    def __call__(self, xs, outs=None, stream=None):
+        if not self._handle:
+            raise RuntimeError("this Batch has already been closed")
+        n = len(self._ops)
+        if len(xs) != n:
+            raise ValueError(f"expected {n} inputs, got {len(xs)}")
+        if outs is None:
+            outs = [_empty(_shape(x), "complex64", _device_of(x)) for x in xs]
+        px = (ctypes.c_void_p * n)()
+        po = (ctypes.c_void_p * n)()
+        for i, (op, x, y) in enumerate(zip(self._ops, xs, outs)):
+            m = int(lib.mr_x_size(ctypes.byref(op._cfg)))
+            _check_size(x, m, f"xs[{i}]")
+            _check_size(y, m, f"outs[{i}]")
+            px[i] = _ptr(x, f"xs[{i}]", "complex64")
+            po[i] = _ptr(y, f"outs[{i}]", "complex64")
+        check(lib.mr_b200_batch_execute(self._handle, px, po, _stream_ptr(stream)),
+              "mr_b200_batch_execute")
+        return outs
+
+    def close(self) -> None:
+        if self._handle:
+            lib.mr_b200_batch_destroy(self._handle)
+            self._handle = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class CGSolver:

@@ -25,7 +25,11 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 struct mr_aha_plan_s {
@@ -48,9 +52,14 @@ struct mr_aha_plan_s {
     // compile-time-specialised kernels (passes3.cu): tile widths, 0 if none
     int xt3_z_buf, xt3_z_cs, xt3_y_buf, xt3_y_cs;
     int nc3;
+    // y inverse into the z buffer (3-D): its own tile choice, first equal
+    // to the y forward one (the autotuner may separate them)
+    int xts_yi, xt3_yi;
     int nch;         // coils per tile of the half-length pass 3, 0 if none
     int launches;    // kernels per execute (accounting)
 };
+
+static void plan_apply_tuned(mr_aha_plan p);
 
 // Choose the in-place kernels where the lengths allow them.
 static void plan_pick_v2(mr_aha_plan p, size_t lim) {
@@ -70,6 +79,8 @@ static void plan_pick_v2(mr_aha_plan p, size_t lim) {
     if (p->ax[0].small && p->fused) p->nc2 = mr_xbd2_coils(g.m[0], g.L, p->cfg.n_coils, lim);
     p->xt3_z_buf = p->xt3_z_cs = p->xt3_y_buf = p->xt3_y_cs = 0;
     p->nc3 = p->nch = 0;
+    p->xts_yi = p->xts_y_buf;
+    p->xt3_yi = 0;
     if (mr_env_int("MR_AHA_B200_NO_FIXED", 0)) return;
     // tile widths may be forced per axis (tuning): MR_AHA_B200_XT_Z, _XT_Y.
     // The first pass (image x coil maps, short z lines) runs fastest with
@@ -83,6 +94,7 @@ static void plan_pick_v2(mr_aha_plan p, size_t lim) {
     if (p->fused) p->nc3 = mr_fixed_xbd_coils(g.m[0], g.L);
     // pass 3 pads x by cn[0] and crops the same window
     if (p->fused) p->nch = mr_fixed_xbdh_coils(g.m[0], g.n[0], g.L);
+    p->xt3_yi = p->xt3_y_buf;
 }
 
 // ---------------------------------------------------------------------------
@@ -298,6 +310,7 @@ static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
     const int ngroups = (int)mr_cdiv(cfg->n_coils, group);
     const int per = (cfg->n_spatial == 3 ? 2 : 0) + 2 + (p->fused ? 1 : 3);
     p->launches = ngroups * per + (cfg->is_masked ? 1 : 0);
+    plan_apply_tuned(p);
     if (cfg->verbose)
         printf("[mr_aha] plan: %s block multiply, %d coil(s) per group, tiles z %d y %d\n",
                p->fused ? "fused" : "stand-alone", p->group, p->xt_z, p->xt_y);
@@ -570,8 +583,8 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.d_plane = w0_plane;
                 a.d_outer = (int64_t)Ny * Nx;
                 a.d_axis = Nx;
-                rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_BUF, a, p->xts_y_buf, p->xt_y, s,
-                                         p->xt3_y_buf);
+                rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_BUF, a, p->xts_yi, p->xt_y, s,
+                                         p->xt3_yi);
             } else {
                 a.nplane = g.L;
                 a.xs_s = S;
@@ -770,5 +783,190 @@ int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, 
     const int ngroups = (int)mr_cdiv(cfg->n_coils, group);
     const int per = (has_z ? 2 : 0) + 2 + (p->fused ? 1 : 3);
     p->launches = ngroups * per + (cfg->is_masked ? 1 : 0) + 1;
+    return MR_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner
+// ---------------------------------------------------------------------------
+// The tunable choices of a plan: per strided pass the specialised kernel's
+// tile width (xt3 > 0) or the in-place kernel's tile exponent (xts >= 0),
+// and the pass-3 kernel (half-length nch / specialised nc3 / in-place nc2 /
+// ping-pong). The tuner measures full applies, one choice at a time
+// (coordinate descent, one sweep), and keeps each improvement; results are
+// remembered per geometry for later plans in the process.
+
+struct mr_tune_choice {
+    int xt3_z_buf, xts_z_buf, xt3_z_cs, xts_z_cs, xt3_y_buf, xts_y_buf, xt3_yi, xts_yi;
+    int xt3_y_cs, xts_y_cs, nch, nc3, nc2;
+};
+
+static mr_tune_choice tune_get(const mr_aha_plan p) {
+    return {p->xt3_z_buf, p->xts_z_buf, p->xt3_z_cs, p->xts_z_cs, p->xt3_y_buf, p->xts_y_buf,
+            p->xt3_yi,    p->xts_yi,    p->xt3_y_cs, p->xts_y_cs, p->nch,       p->nc3,
+            p->nc2};
+}
+
+static void tune_set(mr_aha_plan p, const mr_tune_choice &c) {
+    p->xt3_z_buf = c.xt3_z_buf;
+    p->xts_z_buf = c.xts_z_buf;
+    p->xt3_z_cs = c.xt3_z_cs;
+    p->xts_z_cs = c.xts_z_cs;
+    p->xt3_y_buf = c.xt3_y_buf;
+    p->xts_y_buf = c.xts_y_buf;
+    p->xt3_yi = c.xt3_yi;
+    p->xts_yi = c.xts_yi;
+    p->xt3_y_cs = c.xt3_y_cs;
+    p->xts_y_cs = c.xts_y_cs;
+    p->nch = c.nch;
+    p->nc3 = c.nc3;
+    p->nc2 = c.nc2;
+}
+
+static std::string tune_key(const mr_aha_plan p) {
+    const mr_geom &g = p->g;
+    char b[256];
+    std::snprintf(b, sizeof(b), "t%d n%d,%d,%d m%d,%d,%d L%d C%d G%d k%d u%d f%d",
+                  p->cfg.traj_type, g.n[0], g.n[1], g.n[2], g.m[0], g.m[1], g.m[2], g.L,
+                  p->cfg.n_coils, p->group, p->cfg.is_masked, g.upper, p->fused);
+    return b;
+}
+
+static std::mutex g_tune_mu;
+static std::map<std::string, mr_tune_choice> g_tuned;
+
+// Tuned choices of an earlier plan of the same geometry, if any.
+static void plan_apply_tuned(mr_aha_plan p) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(tune_key(p));
+    if (it != g_tuned.end()) tune_set(p, it->second);
+}
+
+static int tune_time(mr_aha_plan p, const float2 *x, const float2 *S, const mr_kernel_ref &K,
+                     const int64_t *mask, float2 *out, int reps, cudaEvent_t e0, cudaEvent_t e1,
+                     float *ms) {
+    cudaStream_t s = p->stream;
+    int rc = mr_plan_execute_k(p, x, S, K, mask, out, s);
+    if (rc != MR_SUCCESS) return rc;
+    MR_CUDA_TRY(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; ++r) {
+        rc = mr_plan_execute_k(p, x, S, K, mask, out, s);
+        if (rc != MR_SUCCESS) return rc;
+    }
+    MR_CUDA_TRY(cudaEventRecord(e1, s));
+    MR_CUDA_TRY(cudaEventSynchronize(e1));
+    float t = 0.f;
+    MR_CUDA_TRY(cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / reps;
+    return MR_SUCCESS;
+}
+
+int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_kernel_ref &K,
+                     const int64_t *mask, float2 *out, int reps, float *best_ms) {
+    if (reps < 1) reps = 1;
+    const mr_geom &g = p->g;
+    const bool has_z = p->cfg.n_spatial == 3;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        cudaGetLastError();
+        if (e0) cudaEventDestroy(e0);
+        MR_FAIL(MR_ERR_CUDA, "autotune: cannot create events");
+    }
+    mr_tune_choice best = tune_get(p);
+    float best_t = 0.f;
+    int rc = tune_time(p, x, S, K, mask, out, reps, e0, e1, &best_t);
+    auto trial = [&](const mr_tune_choice &c) {
+        if (rc != MR_SUCCESS) return;
+        tune_set(p, c);
+        float t = 0.f;
+        rc = tune_time(p, x, S, K, mask, out, reps, e0, e1, &t);
+        if (rc == MR_SUCCESS && t < best_t) {
+            best_t = t;
+            best = c;
+        }
+        tune_set(p, best);
+    };
+    // strided passes: (xt3, xts) fields, axis length, store mode, active
+    struct knob {
+        int mr_tune_choice::*xt3;
+        int mr_tune_choice::*xts;
+        int M, smode;
+        bool on;
+    };
+    const knob knobs[] = {
+        {&mr_tune_choice::xt3_z_buf, &mr_tune_choice::xts_z_buf, g.m[2], MR_SM_BUF, has_z},
+        {&mr_tune_choice::xt3_y_buf, &mr_tune_choice::xts_y_buf, g.m[1], MR_SM_BUF, true},
+        {&mr_tune_choice::xt3_yi, &mr_tune_choice::xts_yi, g.m[1], MR_SM_BUF, has_z},
+        {&mr_tune_choice::xt3_y_cs, &mr_tune_choice::xts_y_cs, g.m[1], MR_SM_COILSUM, !has_z},
+        {&mr_tune_choice::xt3_z_cs, &mr_tune_choice::xts_z_cs, g.m[2], MR_SM_COILSUM, has_z},
+    };
+    const bool fixed_ok = mr_env_int("MR_AHA_B200_NO_FIXED", 0) == 0;
+    // pass 3 first (the largest share), then the strided passes
+    if (p->fused && rc == MR_SUCCESS) {
+        const mr_tune_choice base = best;
+        const int nch0 = fixed_ok ? mr_fixed_xbdh_coils(g.m[0], g.n[0], g.L) : 0;
+        const int nc2_0 = p->ax[0].small && mr_env_int("MR_AHA_B200_FFT_V1", 0) == 0
+                              ? mr_xbd2_coils(g.m[0], g.L, p->cfg.n_coils, (size_t)mr_smem_limit())
+                              : 0;
+        std::vector<mr_tune_choice> cands;
+        if (nch0 > 0) {
+            mr_tune_choice c = base;
+            c.nch = nch0;
+            cands.push_back(c);
+        }
+        int ncs[8];
+        const int nn = fixed_ok ? mr_fixed_xbd_list(g.m[0], g.L, ncs, 8) : 0;
+        for (int i = 0; i < nn; ++i) {
+            mr_tune_choice c = base;
+            c.nch = 0;
+            c.nc3 = ncs[i];
+            cands.push_back(c);
+        }
+        if (nc2_0 > 0) {
+            mr_tune_choice c = base;
+            c.nch = c.nc3 = 0;
+            c.nc2 = nc2_0;
+            cands.push_back(c);
+        }
+        {
+            mr_tune_choice c = base;
+            c.nch = c.nc3 = c.nc2 = 0;
+            cands.push_back(c);
+        }
+        for (const mr_tune_choice &c : cands)
+            if (std::memcmp(&c, &base, sizeof(c)) != 0) trial(c);
+    }
+    for (const knob &k : knobs) {
+        if (!k.on || rc != MR_SUCCESS) continue;
+        const mr_tune_choice base = best;
+        std::vector<mr_tune_choice> cands;
+        int xts[16];
+        const int nf = fixed_ok ? mr_fixed_strided_list(k.M, k.smode, xts, 16) : 0;
+        for (int i = 0; i < nf; ++i) {
+            mr_tune_choice c = base;
+            c.*k.xt3 = xts[i];
+            cands.push_back(c);
+        }
+        const int e0x = base.*k.xts;
+        for (int d = 0; d < 3 && e0x - d >= 0; ++d) {
+            mr_tune_choice c = base;
+            c.*k.xt3 = 0;
+            c.*k.xts = e0x - d;
+            cands.push_back(c);
+        }
+        for (const mr_tune_choice &c : cands)
+            if (std::memcmp(&c, &base, sizeof(c)) != 0) trial(c);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != MR_SUCCESS) return rc;
+    tune_set(p, best);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tuned[tune_key(p)] = best;
+    }
+    if (best_ms) *best_ms = best_t;
+    if (p->cfg.verbose)
+        printf("[mr_aha] autotune %s: %.3f ms per apply\n", tune_key(p).c_str(), best_t);
     return MR_SUCCESS;
 }

@@ -88,6 +88,16 @@ int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s);
 // to the pad window: coils per tile (0 if M != 2 n_in or not instantiated),
 // and its launcher (a.nc set to that).
 int mr_fixed_xbdh_coils(int M, int n_in, int L);
+// Autotuner candidates: every instantiated strided tile width of length M
+// for the store mode, every instantiated coils-per-tile of pass 3 for (M, L),
+// that fit shared memory; return how many were written (at most max).
+int mr_fixed_strided_list(int M, int smode, int *xt, int max);
+int mr_fixed_xbd_list(int M, int L, int *nc, int max);
+// Time candidate kernel choices for every pass with full applies on the
+// given arguments and keep the fastest (also for later plans of the same
+// geometry in this process). *best_ms: the tuned apply's time.
+int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_kernel_ref &K,
+                     const int64_t *mask, float2 *out, int reps, float *best_ms);
 int mr_launch_xbdh(const mr_x_args &a, cudaStream_t s);
 int mr_xbd2_coils(int M, int L, int ncoil, size_t limit);
 int mr_xbd2_stride(int M);

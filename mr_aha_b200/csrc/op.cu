@@ -455,6 +455,39 @@ extern "C" int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d
     return rc;
 }
 
+extern "C" int mr_b200_op_autotune(mr_op op, int reps, float *ms) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_autotune: op is NULL");
+    MR_REQUIRE(reps >= 1 && reps <= 100, "mr_b200_op_autotune: reps = %d outside [1, 100]", reps);
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
+    const size_t vb = (size_t)mr_x_size(&op->cfg) * sizeof(float2);
+    float2 *buf = nullptr;
+    int rc = MR_SUCCESS;
+    if (cudaMalloc(&buf, 2 * vb) != cudaSuccess) {
+        cudaGetLastError();
+        buf = nullptr;
+        mr_set_error("mr_b200_op_autotune: cannot allocate 2 x %zu bytes of trial vectors", vb);
+        rc = MR_ERR_ALLOC;
+    }
+    // a constant non-zero trial input (timings do not depend on the values)
+    if (rc == MR_SUCCESS && cudaMemsetAsync(buf, 0x3c, 2 * vb, op->stream) != cudaSuccess) {
+        cudaGetLastError();
+        mr_set_error("mr_b200_op_autotune: cudaMemsetAsync failed");
+        rc = MR_ERR_CUDA;
+    }
+    if (rc == MR_SUCCESS)
+        rc = mr_plan_autotune(op->plan, buf, op->S, op_kernel_ref(op), op->mask,
+                              buf + vb / sizeof(float2), reps, ms);
+    if (buf) {
+        cudaStreamSynchronize(op->stream);
+        cudaFree(buf);
+    }
+    if (prev != op->dev) cudaSetDevice(prev);
+    return rc;
+}
+
 extern "C" int mr_b200_op_launches(mr_op op, int *n) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");

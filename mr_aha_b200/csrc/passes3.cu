@@ -456,3 +456,28 @@ int mr_launch_xbdh(const mr_x_args &a, cudaStream_t s) {
 #undef MR_XH_CASE
     MR_FAIL(MR_ERR_INTERNAL, "no half-length block-diagonal pass for N = %d, L = %d", N, a.L);
 }
+
+int mr_fixed_strided_list(int M, int smode, int *xt, int max) {
+    // every instantiated tile width of this length that fits the per-block
+    // shared memory limit, for the autotuner
+    int n = 0;
+#define MR_S3_LISTPICK(m, w)                                                                \
+    if (M == m && n < max &&                                                                \
+        (size_t)m * w * sizeof(float2) * (smode == MR_SM_COILSUM ? 2 : 1) <=                \
+            (size_t)mr_smem_limit())                                                        \
+        xt[n++] = w;
+    MR_S3_LIST(MR_S3_LISTPICK)
+#undef MR_S3_LISTPICK
+    return n;
+}
+
+int mr_fixed_xbd_list(int M, int L, int *nc, int max) {
+    int n = 0;
+#define MR_X3_LISTPICK(m, l, c)                                                             \
+    if (M == m && L == l && n < max &&                                                      \
+        (size_t)c * l * odd_stride<m>() * sizeof(float2) <= (size_t)mr_smem_limit())        \
+        nc[n++] = c;
+    MR_X3_LIST(MR_X3_LISTPICK)
+#undef MR_X3_LISTPICK
+    return n;
+}
