@@ -37,6 +37,11 @@ MR_EXPORT int mr_b200_op_kernel_format(mr_op op, int *format);
 MR_EXPORT int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_AhAx,
                                  float *ms, char *names, int max_passes, int *n_passes);
 
+/* No reference counterpart. Device memory the operator holds (its owned
+ * kernel copies, 16-bit kernel and scales, owned maps / mask, plan work
+ * buffers); borrowed arrays are not counted. */
+MR_EXPORT int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes);
+
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 
@@ -118,6 +123,13 @@ MR_EXPORT int mr_b200_cg_create(mr_op op, const mr_complex *d_b, mr_complex *d_x
  * solver's own stream, ordered after earlier work on the operator's stream and
  * before later work there. Returns without waiting for the GPU. */
 MR_EXPORT int mr_b200_cg_step(mr_b200_cg cg, int n_iter);
+
+/* *busy = 1 while iterations issued on the solver's stream are still
+ * running on the GPU, else 0. Does not wait. */
+MR_EXPORT int mr_b200_cg_busy(mr_b200_cg cg, int *busy);
+
+/* Iterations issued so far (host-side count, including the ones in flight). */
+MR_EXPORT int mr_b200_cg_iterations(mr_b200_cg cg, int *n);
 
 /* Wait for the solver and copy |r_k|^2 for k = 0 .. min(iterations, max_iters)
  * (at most `max` values) to host `rr`; *n receives how many exist. */

@@ -526,6 +526,15 @@ class AhAOp:
         return float(ms.value)
 
     @property
+    def device_bytes(self) -> int:
+        """Device memory held by the operator (``mr_b200_op_device_bytes``)."""
+        self._check_open()
+        b = ctypes.c_uint64(0)
+        check(lib.mr_b200_op_device_bytes(self._handle, ctypes.byref(b)),
+              "mr_b200_op_device_bytes")
+        return int(b.value)
+
+    @property
     def launches_per_apply(self) -> int:
         self._check_open()
         n = ctypes.c_int(0)
@@ -727,6 +736,22 @@ class CGSolver:
         if not self._handle:
             raise RuntimeError("this CGSolver has already been closed")
         check(lib.mr_b200_cg_step(self._handle, int(n)), "mr_b200_cg_step")
+
+    @property
+    def busy(self) -> bool:
+        """True while issued iterations are still running (does not wait)."""
+        if not self._handle:
+            return False
+        v = ctypes.c_int(0)
+        check(lib.mr_b200_cg_busy(self._handle, ctypes.byref(v)), "mr_b200_cg_busy")
+        return bool(v.value)
+
+    @property
+    def iterations(self) -> int:
+        """Iterations issued so far."""
+        v = ctypes.c_int(0)
+        check(lib.mr_b200_cg_iterations(self._handle, ctypes.byref(v)), "mr_b200_cg_iterations")
+        return int(v.value)
 
     def residuals(self):
         """``|r_k|^2`` for the iterations done so far (waits for the GPU)."""

@@ -200,6 +200,11 @@ static size_t plan_bytes(const mr_aha_plan p, int group) {
     return b;
 }
 
+size_t mr_plan_device_bytes(mr_aha_plan p) {
+    const mr_geom &g = p->g;
+    return plan_bytes(p, p->group) + (size_t)(g.m[0] + g.m[1] + g.m[2]) * sizeof(float2);
+}
+
 static int plan_alloc(mr_aha_plan p, int group) {
     const mr_geom &g = p->g;
     const size_t P = (size_t)group * g.L;

@@ -398,6 +398,33 @@ extern "C" int mr_b200_cg_step(mr_b200_cg cg, int n_iter) {
     return rc;
 }
 
+extern "C" int mr_b200_cg_busy(mr_b200_cg cg, int *busy) {
+    mr_clear_error();
+    MR_REQUIRE(cg != nullptr && busy != nullptr, "mr_b200_cg_busy: NULL argument");
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != cg->dev) MR_CUDA_TRY(cudaSetDevice(cg->dev));
+    const cudaError_t e = cudaStreamQuery(cg->s);
+    if (prev != cg->dev) cudaSetDevice(prev);
+    if (e == cudaSuccess) {
+        *busy = 0;
+    } else if (e == cudaErrorNotReady) {
+        cudaGetLastError();
+        *busy = 1;
+    } else {
+        cudaGetLastError();
+        MR_FAIL(MR_ERR_CUDA, "mr_b200_cg_busy: %s", cudaGetErrorString(e));
+    }
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_b200_cg_iterations(mr_b200_cg cg, int *n) {
+    mr_clear_error();
+    MR_REQUIRE(cg != nullptr && n != nullptr, "mr_b200_cg_iterations: NULL argument");
+    *n = cg->iters;
+    return MR_SUCCESS;
+}
+
 extern "C" int mr_b200_cg_residuals(mr_b200_cg cg, double *rr, int max, int *n) {
     mr_clear_error();
     MR_REQUIRE(cg != nullptr, "mr_b200_cg_residuals: cg is NULL");

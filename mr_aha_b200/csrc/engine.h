@@ -144,6 +144,9 @@ size_t mr_plan_struct_size();
 int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, void *storage,
                              size_t *needed);
 
+// Device bytes a plan holds (work buffers, FFT tables).
+size_t mr_plan_device_bytes(mr_aha_plan p);
+
 // Operator internals shared with the solver (op.cu).
 int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s);
 const mr_config *mr_op_config(mr_op op);

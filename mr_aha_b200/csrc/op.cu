@@ -488,6 +488,21 @@ extern "C" int mr_b200_op_autotune(mr_op op, int reps, float *ms) {
     return rc;
 }
 
+extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && bytes != nullptr, "mr_b200_op_device_bytes: NULL argument");
+    const mr_config *c = &op->cfg;
+    const uint64_t nloc = c->is_masked ? (uint64_t)c->num_masked : (uint64_t)mr_pad_size(c);
+    const uint64_t ntri = (uint64_t)mr_num_tri(c->L);
+    uint64_t b = op->plan ? mr_plan_device_bytes(op->plan) : 0;
+    if (op->K_own) b += nloc * ntri * sizeof(float2);
+    if (op->K16) b += nloc * ntri * 4 + nloc * sizeof(float);
+    if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
+    if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
+    *bytes = b;
+    return MR_SUCCESS;
+}
+
 extern "C" int mr_b200_op_launches(mr_op op, int *n) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");

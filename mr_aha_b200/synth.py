@@ -198,3 +198,52 @@ def workload(name: str, with_x: bool = True) -> dict:
     return dict(traj_type=tt, n_dim=n_dim, phi2_dim=default_phi2_dim(tt, n_dim),
                 L=L, n_coils=nc, traj=traj, phi2=phi2, x=x, SEs=SEs, Phi=Phi,
                 frames=frames)
+
+
+# ---------------------------------------------------------------------------
+# Uneven batches and served requests
+# ---------------------------------------------------------------------------
+
+BATCH_CHOICES = dict(n=(128, 192, 256, 320), nz=(8, 16, 32, 56), L=(4, 8, 16, 32),
+                     coils=(8, 12, 16, 32))
+
+
+def batch_specs(n_ops: int = 48, seed: int = 3, choices: dict = BATCH_CHOICES,
+                spokes=(200, 1000)) -> list:
+    """Seeded stack operators of uneven size: in-plane ``n``, ``Nz``, rank
+    ``L`` and coil count drawn uniformly from ``choices``; spokes uniform in
+    ``spokes``; ``Nkx = 2 n``; ``max(L, spokes // 5)`` frames split evenly."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_ops):
+        n = int(rng.choice(choices["n"]))
+        nz = int(rng.choice(choices["nz"]))
+        L = int(rng.choice(choices["L"]))
+        nc = int(rng.choice(choices["coils"]))
+        n_traj = int(rng.integers(spokes[0], spokes[1] + 1))
+        out.append(dict(traj_type="stack", n_dim=(n, n, nz), L=L, n_coils=nc, n_traj=n_traj,
+                        n_kx=2 * n, n_frames=max(L, n_traj // 5), frame_rule="div",
+                        seed=seed * 1000 + i))
+    return out
+
+
+def spec_inputs(spec: dict, with_x: bool = True) -> dict:
+    """Inputs of one operator spec (same recipe as the headline workloads)."""
+    rng = np.random.default_rng(spec["seed"])
+    tt, n_dim, L, nc = spec["traj_type"], tuple(spec["n_dim"]), spec["L"], spec["n_coils"]
+    traj = make_traj(tt, spec["n_traj"], spec["n_kx"])
+    Phi = make_basis(rng, L, spec["n_frames"])
+    frames = frames_of_spokes(spec["n_traj"], spec["n_frames"], spec["frame_rule"])
+    n_kz = n_dim[2] if tt == "stack" else None
+    phi2 = make_phi2_basis(Phi, frames, n_kz)
+    img = tuple(reversed(n_dim))
+    SEs = make_smooth_maps(rng, nc, img)
+    x = crandn(rng, (L,) + img) if with_x else None
+    return dict(traj_type=tt, n_dim=n_dim, phi2_dim=default_phi2_dim(tt, n_dim), L=L,
+                n_coils=nc, traj=traj, phi2=phi2, x=x, SEs=SEs)
+
+
+def poisson_arrivals(rate: float, n: int, seed: int = 0) -> np.ndarray:
+    """Arrival times (s) of a Poisson process of ``rate`` per second."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
