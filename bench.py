@@ -27,6 +27,7 @@ collective on the data path (``scaling`` = weak).
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -55,6 +56,9 @@ def parse():
                     choices=["complex64", "bf16", "int16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=2)
+    ap.add_argument("--tune", action="store_true", help="batch48: autotune each geometry")
+    ap.add_argument("--requests", type=int, default=12, help="serve: number of requests")
+    ap.add_argument("--rate", type=float, default=2.0, help="serve: arrivals per second")
     return ap.parse_args()
 
 
@@ -373,10 +377,254 @@ def run_ours(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Further workloads (one JSON line each): CG at the headline size, the uneven
+# batch and the serving loop
+# ---------------------------------------------------------------------------
+
+def _rel(a, b) -> float:
+    import torch
+
+    return float(torch.linalg.vector_norm((a - b).to(torch.complex128)) /
+                 torch.linalg.vector_norm(b.to(torch.complex128)))
+
+
+def run_cg(args):
+    """CG on b = A^H A x_true + 1e-3 noise at the headline size, 30
+    iterations from zero, with the kernel stored as complex64, int16 + scale
+    and bf16 + scale; errors against the complex64 operator on the GPU (the
+    FP64-oracle comparison runs at a reduced size in the GPU tests)."""
+    import torch
+
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    wl = synth.workload("stack320")
+    x = torch.from_numpy(wl["x"]).to(dev)
+    S = torch.from_numpy(wl["SEs"]).to(dev)
+    cfg = mr.make_config(wl["traj_type"], wl["n_dim"], wl["L"], phi2_dim=wl["phi2_dim"],
+                         n_coils=wl["n_coils"], mem_fraction=0.6)
+    op = mr.create_op(cfg, S, torch.from_numpy(wl["phi2"]).to(dev),
+                      torch.from_numpy(wl["traj"]).to(dev))
+    ax = op(x)
+    g = torch.Generator(device=dev).manual_seed(7)
+    sigma = 1e-3 * float(torch.linalg.vector_norm(ax)) / (ax.numel() ** 0.5)
+    b = ax + sigma * torch.randn(ax.shape, dtype=ax.dtype, device=dev, generator=g)
+    n_iter = 30
+    reps = max(1, args.steps // 10)
+    res = {}
+    x_c64 = None
+    y_c64 = op(x)
+    for fmt in ("complex64", "int16", "bf16"):
+        op.set_kernel_format(fmt)
+        y = op(x)
+        xs, rr = op.cg(b, n_iter)               # warm-up (graph capture)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            xs, rr = op.cg(b, n_iter)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        if fmt == "complex64":
+            x_c64 = xs.clone()
+        res[fmt] = {"solve_ms": ms, "solves_per_s": 1e3 / ms, "ms_per_iteration": ms / n_iter,
+                    "apply_rel_l2_vs_complex64": _rel(y, y_c64),
+                    "iterate_rel_l2_vs_complex64": _rel(xs, x_c64),
+                    "rr_first_last": [float(rr[0]), float(rr[-1])]}
+    op.close()
+    line = {"metric": "CG solves/s (30 iterations, stack320)",
+            "value": res["int16"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic",
+            "dtype": "c64 vectors, FP64 reductions, int16+scale kernel",
+            "config": {"workload": "stack320 CG", "n_iter": n_iter, "noise": 1e-3,
+                       "reps": reps},
+            "formats": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _op_bytes(spec, fmt):
+    n, _, nz = spec["n_dim"]
+    vpad = (2 * n) * (2 * n) * nz
+    ntri = spec["L"] * (spec["L"] + 1) // 2
+    return vpad * ntri * (8 if fmt == "complex64" else 4) + (0 if fmt == "complex64" else 4 * vpad)
+
+
+def _alg_bytes_spec(spec, fmt):
+    n, _, nz = spec["n_dim"]
+    wl = {"n_dim": spec["n_dim"], "phi2_dim": (2 * n, 2 * n, nz), "L": spec["L"],
+          "n_coils": spec["n_coils"]}
+    kb = 8 if fmt == "complex64" else 4
+    return alg_bytes(wl, kb, 0 if fmt == "complex64" else 4)["apply"]
+
+
+def run_batch(args):
+    """48 uneven operators (random kernels of the right size), admitted in
+    waves by device memory, each wave applied as one batch (worker streams,
+    one captured CUDA graph), complex64 and int16 kernels."""
+    import torch
+
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    specs = synth.batch_specs(48, seed=3)
+    budget = 150e9
+    peak, peak_kind = measured_peak_hbm()
+    steps = max(1, args.steps // 10)
+    out = {}
+    for fmt in ("complex64", "int16"):
+        # waves: resident bytes of the wave plus, for 16-bit kernels, the
+        # largest complex64 kernel alive while it is converted
+        waves, cur, used, trans = [], [], 0.0, 0.0
+        for sp in specs:
+            img = sp["n_dim"][0] * sp["n_dim"][1] * sp["n_dim"][2]
+            need = _op_bytes(sp, fmt) + 8 * img * (sp["n_coils"] + 2 * sp["L"]) + 6e9
+            t = 0.0 if fmt == "complex64" else _op_bytes(sp, "complex64")
+            if cur and used + need + max(trans, t) > budget:
+                waves.append(cur)
+                cur, used, trans = [], 0.0, 0.0
+            cur.append(sp)
+            used += need
+            trans = max(trans, t)
+        if cur:
+            waves.append(cur)
+        t_total, applies, bytes_total, tune_s = 0.0, 0, 0.0, 0.0
+        for wave in waves:
+            ops, keep = [], []
+            for sp in wave:
+                g = torch.Generator(device=dev).manual_seed(sp["seed"])
+                cfg = mr.make_config("stack", sp["n_dim"], sp["L"], n_coils=sp["n_coils"],
+                                     mem_fraction=0.03)
+                img = tuple(reversed(sp["n_dim"]))
+                S = torch.randn((sp["n_coils"],) + img, dtype=torch.complex64, device=dev,
+                                generator=g)
+                K = torch.randn(mr.phi2_toep_shape(cfg), dtype=torch.complex64, device=dev,
+                                generator=g)
+                x = torch.randn((sp["L"],) + img, dtype=torch.complex64, device=dev,
+                                generator=g)
+                # the operator borrows the kernel; after a 16-bit conversion
+                # it lets go of it and the complex64 array is freed
+                op = mr.create_op(cfg, S, None, None, _phi2_toep=K)
+                if fmt != "complex64":
+                    op.set_kernel_format(fmt, keep_complex64=False)
+                del K
+                torch.cuda.empty_cache()
+                ops.append(op)
+                keep.append((S, x))
+            t0 = time.perf_counter()
+            b = mr.Batch(ops, n_streams=4, graph=True, tune=args.tune)
+            tune_s += time.perf_counter() - t0
+            xs = [k[1] for k in keep]
+            ys = [torch.empty_like(v) for v in xs]
+            for _ in range(2):
+                b(xs, ys)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(steps):
+                b(xs, ys)
+            e1.record()
+            torch.cuda.synchronize()
+            t_total += e0.elapsed_time(e1) / 1e3
+            applies += steps * len(wave)
+            bytes_total += steps * sum(_alg_bytes_spec(sp, fmt) for sp in wave)
+            b.close()
+            for op in ops:
+                op.close()
+            del keep, xs, ys
+            torch.cuda.empty_cache()
+        gbs = bytes_total / t_total / 1e9
+        out[fmt] = {"applies_per_s": applies / t_total, "waves": len(waves),
+                    "alg_gbs": gbs, "roofline_frac": gbs / peak, "timed_s": t_total,
+                    "tune_s": tune_s if args.tune else 0.0}
+    line = {"metric": "batched A^H A applies/s (48 uneven operators)",
+            "value": out["int16"]["applies_per_s"], "unit": "applies/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic (random kernels of the right size)",
+            "dtype": "c64", "config": {"workload": "batch48", "seed": 3,
+                                       "budget_gb": budget / 1e9, "steps_per_wave": steps,
+                                       "autotune": bool(args.tune), "peak_gbs": peak,
+                                       "peak_kind": peak_kind},
+            "modes": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_serve(args):
+    """Poisson arrivals of CG requests sized from the uneven-batch
+    distribution; the serving loop (int16 + scale kernel, up to 8 resident
+    solves, 160 GB admission) against the plain complex64 operator one solve
+    at a time, on the same requests."""
+    import torch
+
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import serve, synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    n_req = args.requests
+    specs = synth.batch_specs(n_req, seed=11)
+    arrivals = synth.poisson_arrivals(args.rate, n_req, seed=12)
+    rng = np.random.default_rng(13)
+    reqs = []
+    for i, sp in enumerate(specs):
+        p = synth.spec_inputs(sp, with_x=False)
+        cfg = mr.make_config("stack", p["n_dim"], p["L"], n_coils=p["n_coils"])
+        img = tuple(reversed(p["n_dim"]))
+        b = torch.randn((p["L"],) + img, dtype=torch.complex64, device=dev,
+                        generator=torch.Generator(device=dev).manual_seed(100 + i))
+        reqs.append(serve.Request(rid=i, arrival=float(arrivals[i]), cfg=cfg,
+                                  SEs=torch.from_numpy(p["SEs"]).to(dev),
+                                  phi2=torch.from_numpy(p["phi2"]).to(dev),
+                                  traj=torch.from_numpy(p["traj"]).to(dev), b=b,
+                                  n_iter=int(rng.integers(10, 41))))
+    # warm-up: the first request alone through both paths (kernel loading)
+    first = [dataclasses.replace(reqs[0], arrival=0.0)]
+    serve.Server(serve.GPUBackend("int16"), hbm_budget=160e9).run(first)
+    serve.run_sequential(serve.GPUBackend("complex64", graph=False), first)
+    srv = serve.Server(serve.GPUBackend("int16"), hbm_budget=160e9, max_active=8, chunk=2)
+    t0 = time.perf_counter()
+    served = srv.run(reqs)
+    t_srv = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    seq = serve.run_sequential(serve.GPUBackend("complex64", graph=False), reqs)
+    t_seq = time.perf_counter() - t0
+    st_srv = serve.latency_stats(served)
+    st_seq = serve.latency_stats(seq)
+    line = {"metric": "served CG solves/s", "value": st_srv["solves_per_s"],
+            "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "dtype": "c64 vectors, int16+scale kernel",
+            "config": {"workload": "serve", "requests": n_req, "rate_per_s": args.rate,
+                       "iters": "U{10..40}", "sizes": "uneven-batch distribution, seed 11",
+                       "hbm_budget_gb": 160, "max_active": 8},
+            "served": dict(st_srv, wall_s=t_srv, peak_active=srv.peak_active,
+                           peak_gb=srv.peak_bytes / 1e9),
+            "sequential_complex64": dict(st_seq, wall_s=t_seq)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
+        if args.workload in ("cg320", "batch48", "serve"):
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the reference has no solver, batch or serving loop"}))
+            return 0
         return run_reference(args)
+    if args.workload == "cg320":
+        return run_cg(args)
+    if args.workload == "batch48":
+        return run_batch(args)
+    if args.workload == "serve":
+        return run_serve(args)
     return run_ours(args)
 
 

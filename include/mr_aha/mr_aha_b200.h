@@ -22,8 +22,10 @@ extern "C" {
 
 /* No reference counterpart. Store the operator's kernel in `format` for all
  * later applies (FFTs and arithmetic stay FP32). keep_complex64 = 0 frees the
- * complex64 copy (then mr_op_kernel fails with MR_ERR_UNSUPPORTED and the
- * format cannot be changed again). Synchronous. */
+ * operator's complex64 copy, or, for a kernel borrowed from the caller
+ * (MR_OP_SHARE_PRIMARY), stops referencing it so that the caller may free it;
+ * then mr_op_kernel fails with MR_ERR_UNSUPPORTED and the format cannot be
+ * changed again. Synchronous. */
 MR_EXPORT int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_complex64);
 
 /* No reference counterpart. Current kernel format of the operator. */

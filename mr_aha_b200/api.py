@@ -507,6 +507,9 @@ class AhAOp:
         check(lib.mr_b200_op_set_kernel_format(self._handle, KERNEL_FORMATS[fmt],
                                                1 if keep_complex64 else 0),
               "mr_b200_op_set_kernel_format")
+        if not keep_complex64 and fmt != "complex64" and len(self._keep) == 3:
+            # a borrowed complex64 kernel is no longer referenced by the library
+            self._keep = (self._keep[0], self._keep[1], None)
 
     @property
     def kernel_format(self) -> str:

@@ -31,11 +31,40 @@ struct mr_kernel_ref {
     int kf;
 };
 
+// An int16 (re, im) pair as two exact floats without conversion
+// instructions: with the sign bit flipped, a code c reads as the unsigned
+// 16-bit u = c + 2^15; placed in the low mantissa bits of 2^23 it forms the
+// float 2^23 + u, and subtracting 2^23 + 2^15 leaves c exactly.
+__device__ __forceinline__ float2 mr_i16x2_to_float2(uint32_t w) {
+    const uint32_t t = w ^ 0x80008000u;
+    const float lo = __uint_as_float(__byte_perm(t, 0x4B000000u, 0x7610)) - 8421376.0f;
+    const float hi = __uint_as_float(__byte_perm(t, 0x4B000000u, 0x7632)) - 8421376.0f;
+    return make_float2(lo, hi);
+}
+
+// A bfloat16 (re, im) pair as two floats (the bf16 bits are the high half
+// of the float's).
+__device__ __forceinline__ float2 mr_bf16x2_to_float2(uint32_t w) {
+    return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xFFFF0000u));
+}
+
 template <int KF>
 struct mr_kload {
     const void *base;
     int64_t stride;
     float s;
+    // element t without the location's scale (16-bit formats: the stored
+    // code; the caller scales the block's result once)
+    __device__ __forceinline__ float2 get_raw(int t) const {
+        if constexpr (KF == MR_KF_F32) {
+            return __ldg(reinterpret_cast<const float2 *>(base) + (int64_t)t * stride);
+        } else {
+            const uint32_t w =
+                __ldg(reinterpret_cast<const unsigned int *>(base) + (int64_t)t * stride);
+            if constexpr (KF == MR_KF_BF16) return mr_bf16x2_to_float2(w);
+            else return mr_i16x2_to_float2(w);
+        }
+    }
     __device__ __forceinline__ float2 get(int t) const {
         if constexpr (KF == MR_KF_F32) {
             return __ldg(reinterpret_cast<const float2 *>(base) + (int64_t)t * stride);
@@ -71,7 +100,9 @@ __device__ __forceinline__ mr_kload<KF> mr_kload_at(const mr_kernel_ref &k, int6
 
 // y[k] = v[k] A for NC vectors of compile-time rank L, walking the packed
 // triangle once. All register indices are compile-time constants after
-// unrolling.
+// unrolling. A 16-bit block is multiplied in its stored codes and the result
+// scaled once by the location's scale (one multiply per output instead of
+// one per element).
 template <int L, int NC, int KF>
 __device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[NC][L],
                                          const mr_kload<KF> &kl, int upper) {
@@ -85,7 +116,7 @@ __device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[N
         for (int c = 0; c < L; ++c) {
 #pragma unroll
             for (int r = c; r < L; ++r) {
-                const float2 a = kl.get(t++);
+                const float2 a = kl.get_raw(t++);
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
                     y[k][c] = c_add(y[k][c], c_mul(a, v[k][r]));
@@ -98,7 +129,7 @@ __device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[N
         for (int c = 0; c < L; ++c) {
 #pragma unroll
             for (int r = 0; r <= c; ++r) {
-                const float2 a = kl.get(t++);
+                const float2 a = kl.get_raw(t++);
 #pragma unroll
                 for (int k = 0; k < NC; ++k) {
                     y[k][c] = c_add(y[k][c], c_mul(a, v[k][r]));
@@ -106,6 +137,65 @@ __device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[N
                 }
             }
         }
+    }
+    if constexpr (KF != MR_KF_F32) {
+#pragma unroll
+        for (int k = 0; k < NC; ++k)
+#pragma unroll
+            for (int i = 0; i < L; ++i) y[k][i] = c_scale(y[k][i], kl.s);
+    }
+}
+
+// Stored index of element (r, c) of a packed L x L triangle (r >= c in the
+// lower packing, r <= c in the upper one).
+template <int L, bool UPPER>
+__host__ __device__ constexpr int bd_t(int r, int c) {
+    return UPPER ? c * (c + 1) / 2 + r : c * L - c * (c - 1) / 2 + (r - c);
+}
+
+// A_rc of a Hermitian block: the stored element, or the conjugate of the
+// stored A_cr (unscaled 16-bit codes for 16-bit formats).
+template <int L, bool UPPER, int KF>
+__device__ __forceinline__ float2 bd_a(const mr_kload<KF> &kl, int r, int c) {
+    const bool stored = UPPER ? (r <= c) : (r >= c);
+    return stored ? kl.get_raw(bd_t<L, UPPER>(r, c)) : c_conj(kl.get_raw(bd_t<L, UPPER>(c, r)));
+}
+
+// Outputs y_c, c in [16 H, 16 H + 16), of y = v A for a rank-32 block, with
+// v_r at vl[r * vs] (shared memory): first the diagonal 16 x 16 block, with
+// this half of v in registers and each stored pair read once, then the
+// off-diagonal block, streaming the other half of v. Two threads (H = 0, 1)
+// cover one block, each reading 136 + 256 of its 528 elements and doing half
+// of its multiply-adds; each needs 64 registers of vectors instead of 128.
+template <int H, bool UPPER, int KF>
+__device__ __forceinline__ void bd_half32(const float2 *vl, int vs, const mr_kload<KF> &kl,
+                                          float2 (&y)[16]) {
+    constexpr int O = 16 * H, P = 16 - O;
+    float2 v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        v[i] = vl[(O + i) * vs];
+        y[i] = make_float2(0.f, 0.f);
+    }
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+#pragma unroll
+        for (int r = c; r < 16; ++r) {
+            const float2 a = bd_a<32, UPPER, KF>(kl, O + r, O + c);
+            y[c] = c_add(y[c], c_mul(a, v[r]));
+            if (r != c) y[r] = c_add(y[r], c_mulc(a, v[c]));
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const float2 vr = vl[(P + r) * vs];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            y[c] = c_add(y[c], c_mul(bd_a<32, UPPER, KF>(kl, P + r, O + c), vr));
+    }
+    if constexpr (KF != MR_KF_F32) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) y[i] = c_scale(y[i], kl.s);
     }
 }
 

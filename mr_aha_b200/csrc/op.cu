@@ -395,8 +395,10 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
                 mr_set_error("kernel quantisation failed");
             } else {
                 op->kf = format == MR_B200_KF_INT16 ? MR_KF_I16 : MR_KF_BF16;
-                if (!keep_complex64 && op->K_own) {
-                    cudaFree(op->K_own);
+                if (!keep_complex64) {
+                    // an owned copy is freed; a borrowed kernel is handed
+                    // back (the caller may free it)
+                    if (op->K_own) cudaFree(op->K_own);
                     op->K_own = nullptr;
                     op->K = nullptr;
                 }

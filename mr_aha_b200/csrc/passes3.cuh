@@ -1,0 +1,445 @@
+// Kernel templates of the compile-time-specialised passes (fftfix.cuh) and
+// the lists of instantiated configurations. The instantiations are spread
+// over several translation units (passes3.cu, p3_*.cu) so that they compile
+// in parallel; passes3.cu dispatches to them.
+#pragma once
+
+#include "engine.h"
+#include "fftfix.cuh"
+
+namespace {
+
+// Block sizes: 512 threads for tiles of more than 10240 elements (one CTA per
+// SM), 256 threads for smaller tiles, with registers capped so that two
+// independent CTAs share an SM (one loads or stores while the other computes).
+
+template <int DIR, int LM, int SM, int M, int XT, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_strided3(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int TILE = M * XT;
+    float2 *acc = sm + TILE;
+    int64_t bid = blockIdx.x;
+    const int plane = (int)(bid % a.nplane);
+    bid /= a.nplane;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int ncl = (SM == MR_SM_COILSUM) ? a.ncoil : 1;
+    const int64_t off0 = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
+    for (int cc = 0; cc < ncl; ++cc) {
+        const int sp = (SM == MR_SM_COILSUM) ? cc * a.L + plane : plane;
+        const float2 *srcp = nullptr, *xp = nullptr, *sp_s = nullptr;
+        if constexpr (LM == MR_LM_BUF) {
+            srcp = a.src + (int64_t)sp * a.s_plane + off0;
+        } else {
+            xp = a.xs_x + (int64_t)(sp % a.L) * a.img_plane + off0;
+            sp_s = a.xs_s + (int64_t)(a.coil0 + sp / a.L) * a.img_plane + off0;
+        }
+        if constexpr (mrfix::factor(M).n >= 2) {
+            // first pass reads global memory, last pass writes it: the tile
+            // is x-major, so consecutive threads touch consecutive x
+            auto load = [&](int b, int e) -> float2 {
+                int sa = e + a.shift_in;
+                if (sa >= M) sa -= M;
+                float2 v = make_float2(0.f, 0.f);
+                if (b < nx && sa < a.n_in) {
+                    const int64_t o = (int64_t)sa * a.s_axis + b;
+                    if constexpr (LM == MR_LM_BUF) v = srcp[o];
+                    else v = c_mul(__ldg(sp_s + o), __ldg(xp + o));
+                }
+                return v;
+            };
+            auto store = [&](int b, int q, float2 v) {
+                int da = q + a.shift_out;
+                if (da >= M) da -= M;
+                if (da < a.n_out && b < nx) {
+                    if constexpr (SM == MR_SM_BUF) {
+                        a.dst[(int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + b] =
+                            c_scale(v, a.scale);
+                    } else {
+                        const float2 w = c_mulc(
+                            __ldg(a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0 +
+                                  (int64_t)da * a.d_axis + b),
+                            v);
+                        const int ai = da * XT + b;
+                        acc[ai] = (cc == 0) ? w : c_add(acc[ai], w);
+                    }
+                }
+            };
+            mrfix::fft_io<true, true, DIR, M, XT, XT, 1, kNT>(sm, a.ax.tw, load, store);
+            __syncthreads();
+            continue;
+        }
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < TILE; idx += kNT) {
+            const int j = idx / XT;
+            const int xx = idx % XT;
+            int sa = j + a.shift_in;
+            if (sa >= M) sa -= M;
+            float2 v = make_float2(0.f, 0.f);
+            if (xx < nx && sa < a.n_in) {
+                const int64_t o = (int64_t)sa * a.s_axis + xx;
+                if constexpr (LM == MR_LM_BUF) v = srcp[o];
+                else v = c_mul(__ldg(sp_s + o), __ldg(xp + o));
+            }
+            sm[idx] = v;
+        }
+        __syncthreads();
+        mrfix::fft<DIR, M, XT, XT, 1, kNT>(sm, a.ax.tw);
+#pragma unroll 4
+        for (int idx = threadIdx.x; idx < a.n_out * XT; idx += kNT) {
+            const int da = idx / XT;
+            const int xx = idx % XT;
+            int q = da - a.shift_out;
+            if (q < 0) q += M;
+            const float2 v = sm[q * XT + xx];
+            if constexpr (SM == MR_SM_BUF) {
+                if (xx < nx)
+                    a.dst[(int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + xx] =
+                        c_scale(v, a.scale);
+            } else {
+                float2 w = make_float2(0.f, 0.f);
+                if (xx < nx)
+                    w = c_mulc(__ldg(a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0 +
+                                     (int64_t)da * a.d_axis + xx),
+                               v);
+                acc[idx] = (cc == 0) ? w : c_add(acc[idx], w);
+            }
+        }
+        __syncthreads();
+    }
+    if constexpr (SM == MR_SM_COILSUM) {
+        for (int idx = threadIdx.x; idx < a.n_out * XT; idx += kNT) {
+            const int da = idx / XT;
+            const int xx = idx % XT;
+            if (xx < nx) {
+                float2 *o = a.dst + (int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + xx;
+                const float2 v = c_scale(acc[idx], a.scale);
+                *o = a.accumulate ? c_add(*o, v) : v;
+            }
+        }
+    }
+}
+
+template <int M>
+constexpr int odd_stride() {
+    return (M % 2 == 0) ? M + 1 : M + 2;
+}
+
+template <int M, int L, int NC, int KF, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__ mr_x_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int LS = odd_stride<M>();
+    constexpr int NL = NC * L;
+    const int chunk = (int)(blockIdx.x % a.nchunk);
+    const int loc = (int)(blockIdx.x / a.nchunk);
+    const int jy = loc % a.My;
+    const int jz = loc / a.My;
+    const int c0 = chunk * NC;
+    const int ncoils = min(NC, a.ncoil - c0);
+    const int64_t pbase = (int64_t)c0 * L;
+    const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
+    const int64_t rstride = a.plane_rows * a.s_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < NL * M; idx += kNT) {
+        const int b = idx / M;
+        const int j = idx - b * M;
+        int sa = j + a.shift_in;
+        if (sa >= M) sa -= M;
+        float2 v = make_float2(0.f, 0.f);
+        if (b < ncoils * L && sa < a.n_in) v = src[b * rstride + sa];
+        sm[b * LS + j] = v;
+    }
+    __syncthreads();
+    mrfix::fft<-1, M, NL, 1, LS, kNT>(sm, a.ax.tw);
+    const int ky = mr_nat2cent_d(jy, a.My, a.cmy);
+    const int kz = mr_nat2cent_d(jz, a.Mz, a.cmz);
+    constexpr int GW = 32 / NC;
+    constexpr int ITEMS = NC * ((M + GW - 1) / GW) * GW;
+    for (int w = threadIdx.x; w < ITEMS; w += kNT) {
+        const int lane = w & 31;
+        const int k = lane / GW;
+        const int jx = (w >> 5) * GW + (lane - k * GW);
+        if (jx >= M || k >= ncoils) continue;
+        float2 v[1][L], y[1][L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[0][l] = sm[(k * L + l) * LS + jx];
+        bool zero = false;
+        int64_t row;
+        if (a.K.inv) {
+            const int r = __ldg(a.K.inv + jx + (int64_t)M * (jy + (int64_t)a.My * jz));
+            zero = r < 0;
+            row = zero ? 0 : r;
+        } else {
+            row = mr_nat2cent_d(jx, M, a.cmx) + (int64_t)M * (ky + (int64_t)a.My * kz);
+        }
+        if (zero) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
+        } else {
+            const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
+            bd_block<L, 1, KF>(v, y, kl, a.upper);
+        }
+#pragma unroll
+        for (int l = 0; l < L; ++l) sm[(k * L + l) * LS + jx] = y[0][l];
+    }
+    __syncthreads();
+    mrfix::fft<1, M, NL, 1, LS, kNT>(sm, a.ax.tw);
+    float2 *dst = a.dst + (pbase * a.plane_rows + loc) * a.d_row;
+    const int64_t dstride = a.plane_rows * a.d_row;
+    for (int idx = threadIdx.x; idx < ncoils * L * a.n_out; idx += kNT) {
+        const int b = idx / a.n_out;
+        const int da = idx - b * a.n_out;
+        int q = da - a.shift_out;
+        if (q < 0) q += M;
+        dst[b * dstride + da] = c_scale(sm[b * LS + q], a.scale);
+    }
+}
+
+// Pass 3 when the transform length is M = 2N, the row holds N samples (zero
+// padding to M) and the output is cropped to the same window. The pad and
+// crop phase ramps then cancel (the block multiply is diagonal in k), and
+// with t[n] = W_M^n (W_M = exp(-2 pi i / M)):
+//   X[2m] = FFT_N(x)[m],  X[2m+1] = FFT_N(x t)[m],
+//   y[n]  = IFFT_N(Z_even)[n] + conj(t[n]) IFFT_N(Z_odd)[n],
+// four length-N transforms of N-sample lines in place of two length-M
+// transforms of half-empty ones. Row b = (coil, rank) of the tile keeps its
+// even half-spectrum in line 2b and its odd one in line 2b + 1.
+template <int N, int L, int NC, int KF, int kNT>
+__global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__ mr_x_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int LS = odd_stride<N>();
+    constexpr int NR = NC * L;
+    constexpr int NL = 2 * NR;
+    const int chunk = (int)(blockIdx.x % a.nchunk);
+    const int loc = (int)(blockIdx.x / a.nchunk);
+    const int jy = loc % a.My;
+    const int jz = loc / a.My;
+    const int c0 = chunk * NC;
+    const int ncoils = min(NC, a.ncoil - c0);
+    const int nrow = ncoils * L;
+    const int64_t pbase = (int64_t)c0 * L;
+    const float2 *tw = a.ax.tw;  // W_M^e, e < M
+    const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
+    const int64_t rstride = a.plane_rows * a.s_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < NR * N; idx += kNT) {
+        const int b = idx / N;
+        const int n = idx - b * N;
+        float2 v = make_float2(0.f, 0.f);
+        if (b < nrow) v = src[b * rstride + n];
+        sm[(2 * b) * LS + n] = v;
+        sm[(2 * b + 1) * LS + n] = c_mul(v, __ldg(tw + n));
+    }
+    __syncthreads();
+    mrfix::fft<-1, N, NL, 1, LS, kNT, 2>(sm, tw);
+    const int ky = mr_nat2cent_d(jy, a.My, a.cmy);
+    const int kz = mr_nat2cent_d(jz, a.Mz, a.cmz);
+    // a warp takes 16 consecutive m of one coil in both parities: lanes 0-15
+    // the even k = 2m, lanes 16-31 the odd k = 2m + 1 (each half-warp reads
+    // 16 consecutive words of one line)
+    constexpr int MB = (N + 15) / 16;
+    if constexpr (L > 16) {
+        // rank 32: two threads per (k, coil), in paired warps (2j: outputs
+        // 0-15, 2j + 1: outputs 16-31); both read v before either writes y
+        static_assert(L == 32 && (kNT / 32) % 2 == 0, "split block multiply is for rank 32");
+        constexpr int ITEMS2 = NC * MB * 2 * 32;
+        constexpr int NIT = (ITEMS2 + kNT - 1) / kNT;
+        for (int it = 0; it < NIT; ++it) {
+            const int w = threadIdx.x + it * kNT;
+            const int lane = w & 31;
+            const int h = (w >> 5) & 1;
+            const int wi = w >> 6;
+            const int k = wi / MB;
+            const int m = (wi - k * MB) * 16 + (lane & 15);
+            const int par = lane >> 4;
+            const bool ok = w < ITEMS2 && m < N && k < ncoils;
+            float2 *line = sm + (2 * k * L + par) * LS + m;
+            float2 y[16];
+            if (ok) {
+                const int jx = 2 * m + par;
+                bool zero = false;
+                int64_t row;
+                if (a.K.inv) {
+                    const int r =
+                        __ldg(a.K.inv + jx + (int64_t)(2 * N) * (jy + (int64_t)a.My * jz));
+                    zero = r < 0;
+                    row = zero ? 0 : r;
+                } else {
+                    row = mr_nat2cent_d(jx, 2 * N, a.cmx) +
+                          (int64_t)(2 * N) * (ky + (int64_t)a.My * kz);
+                }
+                if (zero) {
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) y[i] = make_float2(0.f, 0.f);
+                } else {
+                    const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
+                    if (a.upper) {
+                        if (h) bd_half32<1, true, KF>(line, 2 * LS, kl, y);
+                        else bd_half32<0, true, KF>(line, 2 * LS, kl, y);
+                    } else {
+                        if (h) bd_half32<1, false, KF>(line, 2 * LS, kl, y);
+                        else bd_half32<0, false, KF>(line, 2 * LS, kl, y);
+                    }
+                }
+            }
+            __syncthreads();
+            if (ok) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) line[2 * (16 * h + i) * LS] = y[i];
+            }
+        }
+    } else {
+    constexpr int ITEMS = NC * MB * 32;
+    for (int w = threadIdx.x; w < ITEMS; w += kNT) {
+        const int lane = w & 31;
+        const int wi = w >> 5;
+        const int k = wi / MB;
+        const int m = (wi - k * MB) * 16 + (lane & 15);
+        const int par = lane >> 4;
+        if (m >= N || k >= ncoils) continue;
+        const int jx = 2 * m + par;
+        float2 *line = sm + (2 * k * L + par) * LS + m;
+        float2 v[1][L], y[1][L];
+#pragma unroll
+        for (int l = 0; l < L; ++l) v[0][l] = line[2 * l * LS];
+        bool zero = false;
+        int64_t row;
+        if (a.K.inv) {
+            const int r = __ldg(a.K.inv + jx + (int64_t)(2 * N) * (jy + (int64_t)a.My * jz));
+            zero = r < 0;
+            row = zero ? 0 : r;
+        } else {
+            row = mr_nat2cent_d(jx, 2 * N, a.cmx) + (int64_t)(2 * N) * (ky + (int64_t)a.My * kz);
+        }
+        if (zero) {
+#pragma unroll
+            for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
+        } else {
+            const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
+            bd_block<L, 1, KF>(v, y, kl, a.upper);
+        }
+#pragma unroll
+        for (int l = 0; l < L; ++l) line[2 * l * LS] = y[0][l];
+    }
+    }
+    __syncthreads();
+    mrfix::fft<1, N, NL, 1, LS, kNT, 2>(sm, tw);
+    float2 *dst = a.dst + (pbase * a.plane_rows + loc) * a.d_row;
+    const int64_t dstride = a.plane_rows * a.d_row;
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < nrow * N; idx += kNT) {
+        const int b = idx / N;
+        const int n = idx - b * N;
+        const float2 e = sm[(2 * b) * LS + n];
+        const float2 o = sm[(2 * b + 1) * LS + n];
+        dst[b * dstride + n] = c_scale(c_add(e, c_mulc(__ldg(tw + n), o)), a.scale);
+    }
+}
+
+template <typename F>
+void set_attr(F *f, unsigned long long &mask) {
+    const int dev = mr_current_device();
+    if (!(mask & (1ull << dev))) {
+        cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, mr_smem_limit());
+        mask |= 1ull << dev;
+    }
+}
+
+template <int DIR, int LM, int SM, int M, int XT>
+int launch_s3(const mr_strided_args &a, cudaStream_t s) {
+    constexpr int kNT = (M * XT > 10240) ? 512 : 256;
+    static unsigned long long attr = 0;
+    set_attr(k_strided3<DIR, LM, SM, M, XT, kNT>, attr);
+    size_t smem = (size_t)M * XT * sizeof(float2);
+    if (SM == MR_SM_COILSUM) smem += (size_t)a.n_out * XT * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
+    if (nblk <= 0) return MR_SUCCESS;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+    k_strided3<DIR, LM, SM, M, XT, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_strided3");
+    return MR_SUCCESS;
+}
+
+template <int M, int L, int NC, int KF>
+int launch_x3(const mr_x_args &a, cudaStream_t s) {
+    constexpr int kNT = (NC * L * M > 10240) ? 512 : 256;
+    static unsigned long long attr = 0;
+    set_attr(k_xbd3<M, L, NC, KF, kNT>, attr);
+    const size_t smem = (size_t)NC * L * odd_stride<M>() * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nloc * a.nchunk;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
+    k_xbd3<M, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_xbd3");
+    return MR_SUCCESS;
+}
+
+template <int N, int L, int NC, int KF>
+int launch_xh(const mr_x_args &a, cudaStream_t s) {
+    constexpr int kNT = (NC * L * 2 * N > 10240) ? 512 : 256;
+    static unsigned long long attr = 0;
+    set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
+    const size_t smem = (size_t)2 * NC * L * odd_stride<N>() * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nloc * a.nchunk;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
+    k_xbdh<N, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    MR_LAUNCH_CHECK("k_xbdh");
+    return MR_SUCCESS;
+}
+
+}  // namespace
+
+// Instantiated strided configurations (length, tile width): list A in
+// passes3.cu, list B in p3_strided_b.cu; each is built in the four modes the
+// plans use. Block-diagonal configurations (length, rank, coils per tile) in
+// passes3.cu; half-length ones (N = M / 2, rank, coils per tile): list A in
+// passes3.cu, B in p3_xbdh_b.cu, C in p3_xbdh_c.cu.
+#define MR_S3_LIST_A(X)                                                                      \
+    X(640, 32) X(640, 16) X(640, 8) X(56, 256) X(56, 128) X(56, 64) X(56, 32) X(56, 16)     \
+    X(128, 64) X(128, 32) X(8, 256)
+#define MR_S3_LIST_B(X)                                                                      \
+    X(512, 32) X(512, 16) X(384, 32) X(384, 16) X(256, 64) X(256, 32) X(256, 16) X(32, 256) \
+    X(32, 128) X(32, 64) X(32, 32) X(16, 256) X(16, 128) X(16, 64) X(16, 32) X(8, 128)
+#define MR_S3_LIST(X) MR_S3_LIST_A(X) MR_S3_LIST_B(X)
+#define MR_X3_LIST(X) X(640, 16, 2) X(640, 16, 1) X(128, 4, 4)
+#define MR_XH_LIST_A(X) X(320, 32, 1) X(320, 16, 1) X(320, 8, 2) X(320, 4, 4)
+#define MR_XH_LIST_B(X)                                                                      \
+    X(256, 32, 1) X(256, 16, 1) X(256, 8, 2) X(256, 4, 4) X(192, 32, 1) X(192, 16, 1)        \
+    X(192, 8, 2) X(192, 4, 4)
+#define MR_XH_LIST_C(X)                                                                      \
+    X(128, 32, 1) X(128, 16, 1) X(128, 8, 2) X(128, 4, 4) X(64, 32, 1) X(64, 16, 1)          \
+    X(64, 8, 2) X(64, 4, 4)
+#define MR_XH_LIST(X) MR_XH_LIST_A(X) MR_XH_LIST_B(X) MR_XH_LIST_C(X)
+
+// Dispatchers of the other translation units: launch when (M, tile) /
+// (N, L, nc) is in their list and set *found, else leave *found false.
+int mr_launch_strided3_b(int dir, int lmode, int smode, const mr_strided_args &a,
+                         cudaStream_t s, bool *found);
+int mr_launch_xbdh_b(const mr_x_args &a, cudaStream_t s, bool *found);
+int mr_launch_xbdh_c(const mr_x_args &a, cudaStream_t s, bool *found);
+
+// Strided dispatch body for one list (used by each translation unit).
+#define MR_S3_DISPATCH(m, xt)                                                                \
+    if (M == m && XT == xt) {                                                                \
+        *found = true;                                                                       \
+        if (dir < 0 && lmode == MR_LM_BUF && smode == MR_SM_BUF)                             \
+            return launch_s3<-1, 0, 0, m, xt>(a, s);                                         \
+        if (dir < 0 && lmode == MR_LM_XS && smode == MR_SM_BUF)                              \
+            return launch_s3<-1, 1, 0, m, xt>(a, s);                                         \
+        if (dir > 0 && lmode == MR_LM_BUF && smode == MR_SM_BUF)                             \
+            return launch_s3<1, 0, 0, m, xt>(a, s);                                          \
+        if (dir > 0 && lmode == MR_LM_BUF && smode == MR_SM_COILSUM)                         \
+            return launch_s3<1, 0, 1, m, xt>(a, s);                                          \
+        MR_FAIL(MR_ERR_INTERNAL, "no specialised strided pass for this mode");              \
+    }
+#define MR_XH_DISPATCH(n, l, c)                                                              \
+    if (N == n && a.L == l && a.nc == c) {                                                   \
+        *found = true;                                                                       \
+        switch (a.K.kf) {                                                                    \
+            case MR_KF_F32: return launch_xh<n, l, c, MR_KF_F32>(a, s);                      \
+            case MR_KF_BF16: return launch_xh<n, l, c, MR_KF_BF16>(a, s);                    \
+            default: return launch_xh<n, l, c, MR_KF_I16>(a, s);                             \
+        }                                                                                    \
+    }

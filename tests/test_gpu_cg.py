@@ -131,9 +131,11 @@ def test_cg_argument_errors():
 
 @pytest.mark.parametrize("fmt", ["int16", "bf16"])
 def test_16bit_operator_equals_dequantized_kernel(fmt):
-    """The device's 16-bit storage holds exactly the values of the oracle's
+    """The device's 16-bit storage holds the values of the oracle's
     restatement: an operator given those values as a complex64 kernel gives
-    the same apply bit for bit."""
+    the same apply up to FP32 rounding (the 16-bit operator multiplies the
+    stored codes and scales each location's result once): relative L2 at
+    most 1e-6."""
     import mr_aha_b200 as mr
 
     w, cfg, K, b, *_ = _problem()
@@ -142,4 +144,4 @@ def test_16bit_operator_equals_dequantized_kernel(fmt):
                                         _phi2_toep=dev(Kq)) as opq:
         y16 = host(op16(dev(b)))
         yq = host(opq(dev(b)))
-    assert np.array_equal(y16, yq)
+    assert O.rel_l2(y16, yq) <= 1e-6

@@ -1,0 +1,64 @@
+"""The instantiated specialised kernels of uneven geometries against the FP64
+oracle: half-length pass 3 for N in {64, 128, 192, 256} and every rank
+configuration (L = 4, 8 with several coils per tile, 16, and 32 with the
+split two-thread block multiply), strided passes of 256 / 384 / 512-point y
+lines and 16 / 32-point z lines; lower and upper packings, a coil count that
+does not fill the last tile, and a masked rank-32 kernel. Tolerance
+(relative L2): 1e-5."""
+
+import numpy as np
+import pytest
+
+from mr_aha_b200 import synth
+from oracle import aha_oracle as O
+from tests.gpu_util import dev, host, random_kernel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+CASES = [
+    ((64, 64, 2), 32, 2, "lower"),
+    ((64, 64, 2), 32, 2, "upper"),
+    ((64, 64, 2), 8, 3, "lower"),
+    ((64, 64, 2), 16, 2, "upper"),
+    ((128, 128, 2), 16, 2, "lower"),
+    ((192, 192, 2), 4, 5, "lower"),
+    ((256, 256, 2), 8, 2, "upper"),
+    ((64, 64, 16), 4, 2, "lower"),
+    ((64, 64, 32), 4, 2, "upper"),
+]
+IDS = [f"{n[0]}x{n[1]}x{n[2]}-L{L}-C{c}-{t}" for n, L, c, t in CASES]
+
+
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_uneven_geometry(case):
+    import mr_aha_b200 as mr
+
+    n_dim, L, nc, tri = case
+    rng = np.random.default_rng(L * 100 + nc)
+    img = tuple(reversed(n_dim))
+    x = synth.crandn(rng, (L,) + img)
+    S = synth.crandn(rng, (nc,) + img)
+    cfg = mr.make_config("stack", n_dim, L, n_coils=nc, triangulation=tri)
+    K = random_kernel(rng, mr.phi2_toep_shape(cfg))
+    y = host(mr.aha_toeplitz(cfg, dev(x), dev(S), dev(K)))
+    ref = O.aha_toeplitz("stack", n_dim, synth.default_phi2_dim("stack", n_dim), L, x, S, K,
+                         upper=tri == "upper")
+    assert O.rel_l2(y, ref) <= TOL, O.rel_l2(y, ref)
+
+
+def test_masked_rank32():
+    import mr_aha_b200 as mr
+
+    n_dim, L, nc = (64, 64, 2), 32, 2
+    rng = np.random.default_rng(77)
+    img = tuple(reversed(n_dim))
+    x = synth.crandn(rng, (L,) + img)
+    S = synth.crandn(rng, (nc,) + img)
+    phi2_dim = synth.default_phi2_dim("stack", n_dim)
+    mask = O.calc_mask("stack", phi2_dim, synth.make_traj("stack", 24, 128), 2)
+    cfg = mr.make_config("stack", n_dim, L, n_coils=nc, is_masked=True, num_masked=len(mask))
+    K = random_kernel(rng, (O.num_tri(L), len(mask)))
+    y = host(mr.aha_toeplitz(cfg, dev(x), dev(S), dev(K), mask=dev(mask)))
+    ref = O.aha_toeplitz("stack", n_dim, phi2_dim, L, x, S, K, mask=mask)
+    assert O.rel_l2(y, ref) <= TOL
