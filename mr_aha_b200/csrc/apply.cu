@@ -43,6 +43,7 @@ struct mr_aha_plan_s {
     float2 *W2, *W3; // unfused pass 3 only: full-grid spectrum in / out
     int *d_inv;      // masked: natural grid index -> mask row
     int fused;       // pass 3 with the block multiply inside
+    int v1_fused;    // the ping-pong fused pass 3 fits shared memory
     int nc_cta;      // coils per CTA in the fused pass 3
     int xt_z, xt_y;  // strided tile widths
     // in-place kernels (passes2.cu): tile exponents per (axis, store mode),
@@ -280,7 +281,11 @@ static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
                 g.m[1], g.m[2]);
     }
     p->nc_cta = 1;
-    p->fused = mr_xbd_smem(g.m[0], g.L, 1) <= lim;
+    // fused pass 3 when a fused kernel fits: the ping-pong one, or the
+    // half-length one (half the shared memory; M = 2N only)
+    p->v1_fused = mr_xbd_smem(g.m[0], g.L, 1) <= lim;
+    p->fused = p->v1_fused || (mr_env_int("MR_AHA_B200_NO_FIXED", 0) == 0 &&
+                               mr_fixed_xbdh_coils(g.m[0], g.n[0], g.L) > 0);
     if (p->fused && g.L <= 16 && mr_xbd_smem(g.m[0], g.L, 2) <= lim && cfg->n_coils >= 2)
         p->nc_cta = 2;
     if (!p->fused && mr_xplain_smem(g.m[0], 1) > lim) {
@@ -526,6 +531,8 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                     a.nchunk = (int)mr_cdiv(G, a.nc);
                     rc = mr_launch_xbd2(a, s);
                 } else {
+                    if (!p->v1_fused)
+                        MR_FAIL(MR_ERR_INTERNAL, "no fused pass-3 kernel fits this geometry");
                     rc = mr_launch_xbd(a, s);
                 }
                 if (rc != MR_SUCCESS) return rc;
@@ -741,6 +748,7 @@ int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, 
                 g.m[1], g.m[2]);
     p->nc_cta = 1;
     p->fused = mr_xbd_smem(g.m[0], g.L, 1) <= lim;
+    p->v1_fused = p->fused;
     if (p->fused && g.L <= 16 && mr_xbd_smem(g.m[0], g.L, 2) <= lim && cfg->n_coils >= 2)
         p->nc_cta = 2;
     if (!p->fused && mr_xplain_smem(g.m[0], 1) > lim)
@@ -933,7 +941,7 @@ int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_k
             c.nc2 = nc2_0;
             cands.push_back(c);
         }
-        {
+        if (p->v1_fused) {
             mr_tune_choice c = base;
             c.nch = c.nc3 = c.nc2 = 0;
             cands.push_back(c);

@@ -82,3 +82,46 @@ def test_sequential_baseline_and_stats():
     assert res[1].admitted >= res[0].finished - 1e-9
     st = serve.latency_stats(res)
     assert st["n"] == 3 and st["p99_s"] >= st["p50_s"] > 0
+
+
+class SlowBuildBackend(FakeBackend):
+    """Building an operator takes `build` seconds of host time."""
+
+    def __init__(self, dt=0.002, build=0.05):
+        super().__init__(dt)
+        self.build = build
+        self.events = []
+
+    def admit(self, req):
+        self.events.append((time.perf_counter(), "admit-start", req.rid))
+        time.sleep(self.build)
+        self.events.append((time.perf_counter(), "admit-end", req.rid))
+        return super().admit(req)
+
+    def step(self, st, n):
+        self.events.append((time.perf_counter(), "step", st["req"].rid))
+        super().step(st, n)
+
+
+def test_background_build_overlaps_running_solves():
+    be = SlowBuildBackend()
+    reqs = _reqs(2, 10, 40, 0.02)
+    srv = serve.Server(be, hbm_budget=100, max_active=4, chunk=1, background=True)
+    res = srv.run(reqs)
+    assert len(res) == 2
+    t_start = next(t for t, e, r in be.events if e == "admit-start" and r == 1)
+    t_end = next(t for t, e, r in be.events if e == "admit-end" and r == 1)
+    during = [t for t, e, r in be.events if e == "step" and r == 0 and t_start < t < t_end]
+    assert during, "request 0 made no progress while request 1 was being built"
+
+
+def test_shortest_remaining_work_first():
+    """A short request arriving while a long one runs finishes first when one
+    solve runs at a time, and both complete."""
+    be = FakeBackend(dt=0.002)
+    reqs = _reqs(2, 10, 5, 0.01)
+    reqs[0].n_iter = 60
+    srv = serve.Server(be, hbm_budget=100, max_active=4, chunk=1, run_slots=1)
+    res = srv.run(reqs)
+    assert res[1].finished < res[0].finished
+    assert [r.rr for r in res] == [[60.0], [5.0]]
