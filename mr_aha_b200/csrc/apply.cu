@@ -84,12 +84,14 @@ static void plan_pick_v2(mr_aha_plan p, size_t lim) {
     p->xt3_yi = 0;
     if (mr_env_int("MR_AHA_B200_NO_FIXED", 0)) return;
     // tile widths may be forced per axis (tuning): MR_AHA_B200_XT_Z, _XT_Y.
-    // The first pass (image x coil maps, short z lines) runs fastest with
-    // narrow tiles: 32 columns of 56-point lines measured 5.2 ms against
-    // 9.4 ms for 256 columns at 320 x 320 x 56, L = 16, 12 coils.
+    // Short z lines run fastest in narrow tiles (small CTAs, four per SM):
+    // 32 columns of 56-point lines measured 5.3 ms (first pass) and 5.2 ms
+    // (last pass) against 9.4 and 8.3 ms for 256 / 128 columns at
+    // 320 x 320 x 56, L = 16, 12 coils.
     const int wz = mr_env_int("MR_AHA_B200_XT_Z", 0), wy = mr_env_int("MR_AHA_B200_XT_Y", 0);
-    p->xt3_z_buf = mr_fixed_strided_xt(g.m[2], MR_SM_BUF, wz ? wz : (g.m[2] <= 64 ? 32 : 0));
-    p->xt3_z_cs = mr_fixed_strided_xt(g.m[2], MR_SM_COILSUM, wz);
+    const int wz0 = wz ? wz : (g.m[2] <= 64 ? 32 : 0);
+    p->xt3_z_buf = mr_fixed_strided_xt(g.m[2], MR_SM_BUF, wz0);
+    p->xt3_z_cs = mr_fixed_strided_xt(g.m[2], MR_SM_COILSUM, wz0);
     p->xt3_y_buf = mr_fixed_strided_xt(g.m[1], MR_SM_BUF, wy);
     p->xt3_y_cs = mr_fixed_strided_xt(g.m[1], MR_SM_COILSUM, wy);
     if (p->fused) p->nc3 = mr_fixed_xbd_coils(g.m[0], g.L);

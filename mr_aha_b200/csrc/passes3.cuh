@@ -13,8 +13,8 @@ namespace {
 // SM), 256 threads for smaller tiles, with registers capped so that two
 // independent CTAs share an SM (one loads or stores while the other computes).
 
-template <int DIR, int LM, int SM, int M, int XT, int kNT>
-__global__ void __launch_bounds__(kNT, 512 / kNT) k_strided3(const __grid_constant__ mr_strided_args a) {
+template <int DIR, int LM, int SM, int M, int XT, int kNT, int MINB>
+__global__ void __launch_bounds__(kNT, MINB) k_strided3(const __grid_constant__ mr_strided_args a) {
     extern __shared__ float2 sm[];
     constexpr int TILE = M * XT;
     float2 *acc = sm + TILE;
@@ -351,14 +351,17 @@ void set_attr(F *f, unsigned long long &mask) {
 template <int DIR, int LM, int SM, int M, int XT>
 int launch_s3(const mr_strided_args &a, cudaStream_t s) {
     constexpr int kNT = (M * XT > 10240) ? 512 : 256;
+    // CTAs per SM the register budget must allow: small tiles need few
+    // registers per thread, so more independent CTAs overlap their phases
+    constexpr int MINB = (M * XT > 10240) ? 1 : (M * XT <= 2048 ? 4 : (M * XT <= 5120 ? 3 : 2));
     static unsigned long long attr = 0;
-    set_attr(k_strided3<DIR, LM, SM, M, XT, kNT>, attr);
+    set_attr(k_strided3<DIR, LM, SM, M, XT, kNT, MINB>, attr);
     size_t smem = (size_t)M * XT * sizeof(float2);
     if (SM == MR_SM_COILSUM) smem += (size_t)a.n_out * XT * sizeof(float2);
     const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
     if (nblk <= 0) return MR_SUCCESS;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
-    k_strided3<DIR, LM, SM, M, XT, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    k_strided3<DIR, LM, SM, M, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
     MR_LAUNCH_CHECK("k_strided3");
     return MR_SUCCESS;
 }
