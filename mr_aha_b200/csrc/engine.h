@@ -88,6 +88,14 @@ int mr_launch_xbd3(const mr_x_args &a, cudaStream_t s);
 // to the pad window: coils per tile (0 if M != 2 n_in or not instantiated),
 // and its launcher (a.nc set to that).
 int mr_fixed_xbdh_coils(int M, int n_in, int L);
+// Half-length strided passes (p3_yhalf.cu) for lines of M = 2N points over N
+// image rows: tile width (`want` if instantiated, else the widest that fits;
+// 0 if none or disabled), instantiated widths, and the launcher (dir -1:
+// rows -> ramp-free spectrum; +1: spectrum -> rows). Forward and inverse are
+// only valid together.
+int mr_half_strided_xt(int N, int want);
+int mr_half_strided_list(int N, int *xt, int max);
+int mr_launch_strided_half(int dir, const mr_strided_args &a, cudaStream_t s);
 // Autotuner candidates: every instantiated strided tile width of length M
 // for the store mode, every instantiated coils-per-tile of pass 3 for (M, L),
 // that fit shared memory; return how many were written (at most max).

@@ -169,13 +169,14 @@ __device__ __forceinline__ void pass_first(float2 *buf, float2 (&u)[UA], const L
 
 // Last pass writing its outputs through store(b, e, v) instead of shared
 // memory (no barrier needed after its reads: shared memory is not written).
-template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int UA, class StoreF>
+template <int R, int DIR, int M, int P, int NL, int ES, int LS, int NT, int TWS, int UA,
+          class StoreF>
 __device__ __forceinline__ void pass_last(const float2 *buf, const float2 *__restrict__ tw,
                                           float2 (&u)[UA], const StoreF &store) {
     constexpr int MR = M / R;
     constexpr int TOTAL = NL * MR;
     constexpr int NB = (TOTAL + NT - 1) / NT;
-    constexpr int TSTEP = M / (P * R);
+    constexpr int TSTEP = TWS * (M / (P * R));
     constexpr bool EXACT = (TOTAL % NT) == 0;
     const int tid = threadIdx.x;
 #pragma unroll
@@ -202,18 +203,18 @@ __device__ __forceinline__ void pass_last(const float2 *buf, const float2 *__res
     }
 }
 
-template <bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, int S, int P, int UA,
-          class StoreF>
+template <bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, int TWS, int S, int P,
+          int UA, class StoreF>
 __device__ __forceinline__ void run_io(float2 *buf, const float2 *tw, float2 (&u)[UA],
                                        const StoreF &store) {
     constexpr radix_list l = factor(M);
     if constexpr (S < l.n) {
         constexpr int R = l.r[S];
         if constexpr (LASTG && S + 1 == l.n) {
-            pass_last<R, DIR, M, P, NL, ES, LS, NT>(buf, tw, u, store);
+            pass_last<R, DIR, M, P, NL, ES, LS, NT, TWS>(buf, tw, u, store);
         } else {
-            pass<R, DIR, M, P, NL, ES, LS, NT, 1>(buf, tw, u);
-            run_io<LASTG, DIR, M, NL, ES, LS, NT, S + 1, P * R>(buf, tw, u, store);
+            pass<R, DIR, M, P, NL, ES, LS, NT, TWS>(buf, tw, u);
+            run_io<LASTG, DIR, M, NL, ES, LS, NT, TWS, S + 1, P * R>(buf, tw, u, store);
         }
     }
 }
@@ -222,13 +223,14 @@ struct no_store {
     __device__ void operator()(int, int, float2) const {}
 };
 
-// Transform of NL lines. FIRSTG: the first pass reads load(b, e) (element e
-// of line b) instead of shared memory. LASTG: the last pass writes
+// Transform of NL lines (twiddle table of TWS times the length, as fft()).
+// FIRSTG: the first pass reads load(b, e) (element e of line b) instead of
+// shared memory. LASTG: the last pass writes
 // store(b, e, v) instead of shared memory (the result is then not in buf;
 // the caller synchronises before reusing buf). Otherwise the result is in
 // buf in natural order.
-template <bool FIRSTG, bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, class LoadF,
-          class StoreF>
+template <bool FIRSTG, bool LASTG, int DIR, int M, int NL, int ES, int LS, int NT, int TWS = 1,
+          class LoadF, class StoreF>
 __device__ __forceinline__ void fft_io(float2 *buf, const float2 *tw, const LoadF &load,
                                        const StoreF &store) {
     constexpr radix_list l = factor(M);
@@ -239,9 +241,9 @@ __device__ __forceinline__ void fft_io(float2 *buf, const float2 *tw, const Load
     if constexpr (FIRSTG) {
         constexpr int R0 = l.r[0];
         pass_first<R0, DIR, M, NL, ES, LS, NT>(buf, u, load);
-        run_io<LASTG, DIR, M, NL, ES, LS, NT, 1, R0>(buf, tw, u, store);
+        run_io<LASTG, DIR, M, NL, ES, LS, NT, TWS, 1, R0>(buf, tw, u, store);
     } else {
-        run_io<LASTG, DIR, M, NL, ES, LS, NT, 0, 1>(buf, tw, u, store);
+        run_io<LASTG, DIR, M, NL, ES, LS, NT, TWS, 0, 1>(buf, tw, u, store);
     }
 }
 

@@ -348,6 +348,104 @@ void set_attr(F *f, unsigned long long &mask) {
     }
 }
 
+// Strided passes of length M = 2N whose input (forward) or output (inverse)
+// is the N image rows, without the zero half: the forward pass computes the
+// ramp-free spectrum X'[k] = sum_n x[n] W_M^{kn} as X'[2m] = FFT_N(x)[m],
+// X'[2m+1] = FFT_N(x t)[m] (t[n] = W_M^n), and the inverse pass
+// y[n] = IFFT_N(Z'_even)[n] + conj(t[n]) IFFT_N(Z'_odd)[n]. Against the
+// padded transforms with pad / crop offset s, X' = W_M^{ks} X and the inverse
+// drops the conjugate ramp, so a forward and an inverse of this kind used
+// together give the same operator (everything between them is diagonal in
+// k). Column b of the tile keeps its even line at b and its odd line at
+// XT + b (x-major layout, element e of line bl at e * 2XT + bl).
+template <int N, int XT, int kNT, int MINB>
+__global__ void __launch_bounds__(kNT, MINB) k_strided_hf(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int NL = 2 * XT;
+    int64_t bid = blockIdx.x;
+    const int plane = (int)(bid % a.nplane);
+    bid /= a.nplane;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const float2 *srcp = a.src + (int64_t)plane * a.s_plane + (int64_t)outer * a.s_outer + x0;
+    float2 *dstp = a.dst + (int64_t)plane * a.d_plane + (int64_t)outer * a.d_outer + x0;
+    const float2 *tw = a.ax.tw;  // W_M^e
+    // each row element is read once and feeds both lines (a plain loop keeps
+    // many loads in flight)
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < N * XT; idx += kNT) {
+        const int e = idx / XT;
+        const int b = idx - e * XT;
+        float2 v = make_float2(0.f, 0.f);
+        if (b < nx) v = srcp[(int64_t)e * a.s_axis + b];
+        sm[e * NL + b] = v;
+        sm[e * NL + XT + b] = c_mul(v, __ldg(tw + e));
+    }
+    __syncthreads();
+    auto store = [&](int bl, int q, float2 v) {
+        const int b = bl % XT;
+        const int k = 2 * q + (bl >= XT ? 1 : 0);
+        if (b < nx) dstp[(int64_t)k * a.d_axis + b] = c_scale(v, a.scale);
+    };
+    mrfix::fft_io<false, true, -1, N, NL, NL, 1, kNT, 2>(sm, tw, [](int, int) {
+        return make_float2(0.f, 0.f); }, store);
+}
+
+template <int N, int XT, int kNT, int MINB>
+__global__ void __launch_bounds__(kNT, MINB) k_strided_hi(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int NL = 2 * XT;
+    int64_t bid = blockIdx.x;
+    const int plane = (int)(bid % a.nplane);
+    bid /= a.nplane;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const float2 *srcp = a.src + (int64_t)plane * a.s_plane + (int64_t)outer * a.s_outer + x0;
+    float2 *dstp = a.dst + (int64_t)plane * a.d_plane + (int64_t)outer * a.d_outer + x0;
+    const float2 *tw = a.ax.tw;
+    auto load = [&](int bl, int e) -> float2 {
+        const int b = bl % XT;
+        const int k = 2 * e + (bl >= XT ? 1 : 0);
+        return b < nx ? srcp[(int64_t)k * a.s_axis + b] : make_float2(0.f, 0.f);
+    };
+    mrfix::fft_io<true, false, 1, N, NL, NL, 1, kNT, 2>(sm, tw, load, mrfix::no_store());
+#pragma unroll 4
+    for (int idx = threadIdx.x; idx < N * XT; idx += kNT) {
+        const int n = idx / XT;
+        const int b = idx - n * XT;
+        if (b < nx) {
+            const float2 e = sm[n * NL + b];
+            const float2 o = sm[n * NL + XT + b];
+            dstp[(int64_t)n * a.d_axis + b] = c_scale(c_add(e, c_mulc(__ldg(tw + n), o)), a.scale);
+        }
+    }
+}
+
+template <int DIR, int N, int XT>
+int launch_sh(const mr_strided_args &a, cudaStream_t s) {
+    constexpr int T = 2 * N * XT;
+    constexpr int kNT = (T > 10240) ? 512 : 256;
+    constexpr int MINB = (T > 10240) ? 1 : (T <= 2048 ? 4 : (T <= 5120 ? 3 : 2));
+    static unsigned long long attr = 0;
+    const size_t smem = (size_t)T * sizeof(float2);
+    const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
+    if (nblk <= 0) return MR_SUCCESS;
+    if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+    if constexpr (DIR < 0) {
+        set_attr(k_strided_hf<N, XT, kNT, MINB>, attr);
+        k_strided_hf<N, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    } else {
+        set_attr(k_strided_hi<N, XT, kNT, MINB>, attr);
+        k_strided_hi<N, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
+    }
+    MR_LAUNCH_CHECK("k_strided_h");
+    return MR_SUCCESS;
+}
+
 template <int DIR, int LM, int SM, int M, int XT>
 int launch_s3(const mr_strided_args &a, cudaStream_t s) {
     constexpr int kNT = (M * XT > 10240) ? 512 : 256;
@@ -415,6 +513,10 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
     X(128, 32, 1) X(128, 16, 1) X(128, 8, 2) X(128, 4, 4) X(64, 32, 1) X(64, 16, 1)          \
     X(64, 8, 2) X(64, 4, 4)
 #define MR_XH_LIST(X) MR_XH_LIST_A(X) MR_XH_LIST_B(X) MR_XH_LIST_C(X)
+
+// Half-length strided passes (N, tile width), in p3_yhalf.cu.
+#define MR_SH_LIST(X) X(320, 16) X(320, 8) X(256, 16) X(256, 8) X(192, 16) X(192, 8) \
+    X(128, 16) X(128, 32) X(64, 32) X(64, 16)
 
 // Dispatchers of the other translation units: launch when (M, tile) /
 // (N, L, nc) is in their list and set *found, else leave *found false.
