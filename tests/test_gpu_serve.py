@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 SMALL = dict(n=(32, 48), nz=(4, 8), L=(2, 4), coils=(2, 4))
 
 
-def _requests(n=6, gap=0.003):
+def _requests(n=6, gap=0.0):
     import mr_aha_b200 as mr
 
     specs = synth.batch_specs(n, seed=9, choices=SMALL, spokes=(24, 64))
@@ -26,7 +26,7 @@ def _requests(n=6, gap=0.003):
         b = synth.crandn(rng, (p["L"],) + tuple(reversed(p["n_dim"])))
         reqs.append(serve.Request(rid=i, arrival=i * gap, cfg=cfg, SEs=dev(p["SEs"]),
                                   phi2=dev(p["phi2"]), traj=dev(p["traj"]), b=dev(b),
-                                  n_iter=int(rng.integers(6, 13))))
+                                  n_iter=int(rng.integers(40, 81))))
     return reqs
 
 
@@ -36,10 +36,11 @@ def test_served_results_equal_alone(fmt):
 
     reqs = _requests()
     srv = serve.Server(serve.GPUBackend(kernel_format=fmt), hbm_budget=40e9, max_active=4,
-                       chunk=2)
+                       chunk=2, run_slots=None)
     res = srv.run(reqs)
     assert [r.rid for r in res] == [r.rid for r in reqs]
-    assert srv.peak_active >= 2
+    # the requests shared the GPU: some request was admitted while another ran
+    assert any(a.admitted < b.admitted < a.finished for a in res for b in res if a is not b)
     for r, q in zip(res, reqs):
         op = mr.create_op(q.cfg, q.SEs, q.phi2, q.traj)
         if fmt != "complex64":
