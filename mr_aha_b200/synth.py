@@ -57,6 +57,13 @@ WORKLOADS = {
                     n_traj=64, n_kx=128, n_frames=32, frame_rule="mod", seed=0),
     "stack320": dict(traj_type="stack", n_dim=(320, 320, 56), L=16, n_coils=12,
                      n_traj=1000, n_kx=640, n_frames=200, frame_rule="div", seed=1),
+    # small cases of the headline kernels for profiling (a few GB on the
+    # device): the headline in-plane size, rank and coils on 4 kz planes; and
+    # the headline 56-point z lines with rank 1 and 16 coils
+    "slab320": dict(traj_type="stack", n_dim=(320, 320, 4), L=16, n_coils=12,
+                    n_traj=1000, n_kx=640, n_frames=200, frame_rule="div", seed=2),
+    "zlines320": dict(traj_type="stack", n_dim=(320, 320, 56), L=1, n_coils=16,
+                      n_traj=1000, n_kx=640, n_frames=200, frame_rule="div", seed=3),
 }
 
 
