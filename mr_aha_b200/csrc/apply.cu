@@ -215,6 +215,10 @@ static size_t plan_bytes(const mr_aha_plan p, int group) {
     return b;
 }
 
+int mr_plan_half_pass3(mr_aha_plan p) {
+    return p->fused && p->nch > 0 && !p->cfg.is_masked && p->g.m[0] % 32 == 0;
+}
+
 size_t mr_plan_device_bytes(mr_aha_plan p) {
     const mr_geom &g = p->g;
     return plan_bytes(p, p->group) + (size_t)(g.m[0] + g.m[1] + g.m[2]) * sizeof(float2);
@@ -420,6 +424,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         MR_LAUNCH_CHECK("k_mask_inverse");
         K.inv = p->d_inv;
         K.stride = nm;
+        K.blk = nullptr;
         prof_mark(prof, "mask_inverse", s);
     } else {
         K.inv = nullptr;

@@ -29,6 +29,10 @@ struct mr_kernel_ref {
     int64_t stride;       // elements between consecutive packed components
     const int *inv;       // masked: natural grid index -> mask row, -1 outside; else NULL
     int kf;
+    // optional complex64 copy in the blocked layout (unmasked, Mx % 32 == 0):
+    // natural grid order, x in blocks of 32, component t of block b at
+    // blk[(b * ntri + t) * 32 + x % 32]; NULL if absent
+    const float2 *blk;
 };
 
 // An int16 (re, im) pair as two exact floats without conversion
@@ -80,6 +84,15 @@ struct mr_kload {
     }
 };
 
+// Loader of one location's block from the blocked layout: `base` points at
+// component 0 of the location, component t is 32 elements further per t (a
+// constant offset once the loop over t is unrolled).
+struct mr_kload_blk {
+    const float2 *base;
+    float s;
+    __device__ __forceinline__ float2 get_raw(int t) const { return __ldg(base + t * 32); }
+};
+
 // Loader for the block of location `loc` (row in the kernel array).
 template <int KF>
 __device__ __forceinline__ mr_kload<KF> mr_kload_at(const mr_kernel_ref &k, int64_t loc) {
@@ -103,9 +116,9 @@ __device__ __forceinline__ mr_kload<KF> mr_kload_at(const mr_kernel_ref &k, int6
 // unrolling. A 16-bit block is multiplied in its stored codes and the result
 // scaled once by the location's scale (one multiply per output instead of
 // one per element).
-template <int L, int NC, int KF>
+template <int L, int NC, int KF, class KL>
 __device__ __forceinline__ void bd_block(const float2 (&v)[NC][L], float2 (&y)[NC][L],
-                                         const mr_kload<KF> &kl, int upper) {
+                                         const KL &kl, int upper) {
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
@@ -155,8 +168,8 @@ __host__ __device__ constexpr int bd_t(int r, int c) {
 
 // A_rc of a Hermitian block: the stored element, or the conjugate of the
 // stored A_cr (unscaled 16-bit codes for 16-bit formats).
-template <int L, bool UPPER, int KF>
-__device__ __forceinline__ float2 bd_a(const mr_kload<KF> &kl, int r, int c) {
+template <int L, bool UPPER, class KL>
+__device__ __forceinline__ float2 bd_a(const KL &kl, int r, int c) {
     const bool stored = UPPER ? (r <= c) : (r >= c);
     return stored ? kl.get_raw(bd_t<L, UPPER>(r, c)) : c_conj(kl.get_raw(bd_t<L, UPPER>(c, r)));
 }
@@ -167,8 +180,8 @@ __device__ __forceinline__ float2 bd_a(const mr_kload<KF> &kl, int r, int c) {
 // off-diagonal block, streaming the other half of v. Two threads (H = 0, 1)
 // cover one block, each reading 136 + 256 of its 528 elements and doing half
 // of its multiply-adds; each needs 64 registers of vectors instead of 128.
-template <int H, bool UPPER, int KF>
-__device__ __forceinline__ void bd_half32(const float2 *vl, int vs, const mr_kload<KF> &kl,
+template <int H, bool UPPER, int KF, class KL>
+__device__ __forceinline__ void bd_half32(const float2 *vl, int vs, const KL &kl,
                                           float2 (&y)[16]) {
     constexpr int O = 16 * H, P = 16 - O;
     float2 v[16];
@@ -181,7 +194,7 @@ __device__ __forceinline__ void bd_half32(const float2 *vl, int vs, const mr_klo
     for (int c = 0; c < 16; ++c) {
 #pragma unroll
         for (int r = c; r < 16; ++r) {
-            const float2 a = bd_a<32, UPPER, KF>(kl, O + r, O + c);
+            const float2 a = bd_a<32, UPPER>(kl, O + r, O + c);
             y[c] = c_add(y[c], c_mul(a, v[r]));
             if (r != c) y[r] = c_add(y[r], c_mulc(a, v[c]));
         }
@@ -191,7 +204,7 @@ __device__ __forceinline__ void bd_half32(const float2 *vl, int vs, const mr_klo
         const float2 vr = vl[(P + r) * vs];
 #pragma unroll
         for (int c = 0; c < 16; ++c)
-            y[c] = c_add(y[c], c_mul(bd_a<32, UPPER, KF>(kl, P + r, O + c), vr));
+            y[c] = c_add(y[c], c_mul(bd_a<32, UPPER>(kl, P + r, O + c), vr));
     }
     if constexpr (KF != MR_KF_F32) {
 #pragma unroll

@@ -154,6 +154,9 @@ int mr_plan_setup_in_scratch(const mr_config *cfg, char *scratch, size_t bytes, 
 
 // Device bytes a plan holds (work buffers, FFT tables).
 size_t mr_plan_device_bytes(mr_aha_plan p);
+// Whether the plan's pass 3 is the half-length kernel on an unmasked grid
+// with Mx % 32 == 0 (it can then read a blocked kernel copy).
+int mr_plan_half_pass3(mr_aha_plan p);
 
 // Operator internals shared with the solver (op.cu).
 int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s);

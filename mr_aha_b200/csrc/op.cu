@@ -27,6 +27,9 @@ struct mr_op_s {
     const int64_t *mask;    // mask (borrowed or owned)
     const float2 *K;        // complex64 kernel, reference layout (borrowed or owned)
     void *S_own, *mask_own, *K_own;
+    // complex64 kernel in the blocked layout read by the half-length pass 3
+    // (mr_kernel_ref::blk), NULL when not built
+    float2 *K_blk;
     // 16-bit kernel copy (MR_B200_KF_BF16 / MR_B200_KF_I16) and its scales
     int kf;
     void *K16;
@@ -42,6 +45,7 @@ static void op_release(mr_op op, int skip_device) {
         if (op->K_own) cudaFree(op->K_own);
         if (op->K16) cudaFree(op->K16);
         if (op->K16_scale) cudaFree(op->K16_scale);
+        if (op->K_blk) cudaFree(op->K_blk);
         cudaGetLastError();
     }
     delete op;
@@ -55,6 +59,62 @@ static int copy_dev(void **dst, const void *src, size_t bytes, cudaStream_t s) {
     }
     MR_CUDA_TRY(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyDeviceToDevice, s));
     return MR_SUCCESS;
+}
+
+// Blocked copy of the complex64 kernel (mr_kernel_ref::blk): natural grid
+// order with x in blocks of 32; element (t, jx, jy, jz) at
+// ((((jz My + jy) Mx/32 + jx/32) ntri + t) 32 + jx % 32), from the centred
+// reference layout K[t Vpad + cent(jx) + Mx (cent(jy) + My cent(jz))].
+__global__ void k_block_kernel(float2 *__restrict__ out, const float2 *__restrict__ K, int Mx,
+                               int My, int Mz, int64_t ntri) {
+    const int64_t vpad = (int64_t)Mx * My * Mz;
+    const int64_t total = vpad * ntri;
+    const int nbx = Mx / 32;
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+         o += (int64_t)gridDim.x * blockDim.x) {
+        const int lane = (int)(o & 31);
+        const int64_t rest = o >> 5;
+        const int64_t t = rest % ntri;
+        const int64_t b = rest / ntri;
+        const int jx = (int)(b % nbx) * 32 + lane;
+        const int64_t yz = b / nbx;
+        const int jy = (int)(yz % My), jz = (int)(yz / My);
+        const int64_t row = mr_nat2cent_d(jx, Mx, Mx / 2) +
+                            (int64_t)Mx * (mr_nat2cent_d(jy, My, My / 2) +
+                                           (int64_t)My * mr_nat2cent_d(jz, Mz, Mz / 2));
+        out[o] = K[t * vpad + row];
+    }
+}
+
+// Build the blocked copy when the operator owns its kernel (a borrowed one
+// may change under it), the plan can use it and the device has room for it
+// (it doubles the complex64 kernel's footprint); otherwise leave it out (the
+// apply then reads the reference layout). Never fails the caller.
+static void op_build_blocked(mr_op op) {
+    if (op->K_blk || !op->K_own || !op->plan || !mr_plan_half_pass3(op->plan) ||
+        mr_env_int("MR_AHA_B200_NO_BLOCKED", 0))
+        return;
+    mr_geom g;
+    mr_geom_from_config(&op->cfg, &g);
+    const int64_t ntri = mr_num_tri(op->cfg.L);
+    const size_t bytes = (size_t)g.vpad * ntri * sizeof(float2);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + ((size_t)2 << 30)) {
+        cudaGetLastError();
+        return;
+    }
+    if (cudaMalloc(&op->K_blk, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        op->K_blk = nullptr;
+        return;
+    }
+    k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1], g.m[2],
+                                                     ntri);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(op->stream) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(op->K_blk);
+        op->K_blk = nullptr;
+    }
 }
 
 static int op_check(const mr_config *cfg, const mr_op_inputs *in, const mr_op_options *o) {
@@ -178,6 +238,7 @@ static int op_create_impl(const mr_config *cfg, const mr_op_inputs *in, const mr
                 cudaGetErrorString(cudaGetLastError()));
     }
     op->kf = MR_KF_F32;
+    op_build_blocked(op);
     mr_op_info_t &inf = op->info;
     inf.method = MR_OP_TOEPLITZ;
     inf.n_devices = 1;
@@ -232,6 +293,7 @@ static mr_kernel_ref op_kernel_ref(mr_op op) {
     std::memset(&K, 0, sizeof(K));
     if (op->kf == MR_KF_F32) {
         K.data = op->K;
+        K.blk = op->K_blk;
     } else {
         K.data = op->K16;
         K.scale = op->K16_scale;
@@ -399,7 +461,9 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
                     // an owned copy is freed; a borrowed kernel is handed
                     // back (the caller may free it)
                     if (op->K_own) cudaFree(op->K_own);
+                    if (op->K_blk) cudaFree(op->K_blk);
                     op->K_own = nullptr;
+                    op->K_blk = nullptr;
                     op->K = nullptr;
                 }
             }
@@ -499,6 +563,7 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     uint64_t b = op->plan ? mr_plan_device_bytes(op->plan) : 0;
     if (op->K_own) b += nloc * ntri * sizeof(float2);
     if (op->K16) b += nloc * ntri * 4 + nloc * sizeof(float);
+    if (op->K_blk) b += nloc * ntri * sizeof(float2);
     if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
     if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
     *bytes = b;

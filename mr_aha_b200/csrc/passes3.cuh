@@ -206,8 +206,10 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__
 //   y[n]  = IFFT_N(Z_even)[n] + conj(t[n]) IFFT_N(Z_odd)[n],
 // four length-N transforms of N-sample lines in place of two length-M
 // transforms of half-empty ones. Row b = (coil, rank) of the tile keeps its
-// even half-spectrum in line 2b and its odd one in line 2b + 1.
-template <int N, int L, int NC, int KF, int kNT>
+// even half-spectrum in line 2b and its odd one in line 2b + 1. BLK: read
+// the complex64 kernel from its blocked copy (a.K.blk, unmasked only), where
+// the 32 frequencies of a warp are contiguous for every component.
+template <int N, int L, int NC, int KF, int kNT, bool BLK = false>
 __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__ mr_x_args a) {
     extern __shared__ float2 sm[];
     constexpr int LS = odd_stride<N>();
@@ -274,6 +276,18 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
                 if (zero) {
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[i] = make_float2(0.f, 0.f);
+                } else if constexpr (BLK) {
+                    constexpr int NTRI = L * (L + 1) / 2;
+                    const mr_kload_blk kl{a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
+                                                        (NTRI * 32) + (2 * (lane & 15) + par),
+                                          1.f};
+                    if (a.upper) {
+                        if (h) bd_half32<1, true, KF>(line, 2 * LS, kl, y);
+                        else bd_half32<0, true, KF>(line, 2 * LS, kl, y);
+                    } else {
+                        if (h) bd_half32<1, false, KF>(line, 2 * LS, kl, y);
+                        else bd_half32<0, false, KF>(line, 2 * LS, kl, y);
+                    }
                 } else {
                     const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
                     if (a.upper) {
@@ -317,6 +331,12 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
         if (zero) {
 #pragma unroll
             for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
+        } else if constexpr (BLK) {
+            constexpr int NTRI = L * (L + 1) / 2;
+            const mr_kload_blk kl{a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
+                                                (NTRI * 32) + (2 * (lane & 15) + par),
+                                  1.f};
+            bd_block<L, 1, KF>(v, y, kl, a.upper);
         } else {
             const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
             bd_block<L, 1, KF>(v, y, kl, a.upper);
@@ -480,11 +500,20 @@ int launch_x3(const mr_x_args &a, cudaStream_t s) {
 template <int N, int L, int NC, int KF>
 int launch_xh(const mr_x_args &a, cudaStream_t s) {
     constexpr int kNT = (NC * L * 2 * N > 10240) ? 512 : 256;
-    static unsigned long long attr = 0;
-    set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
     const size_t smem = (size_t)2 * NC * L * odd_stride<N>() * sizeof(float2);
     const int64_t nblk = (int64_t)a.nloc * a.nchunk;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
+    if constexpr (KF == MR_KF_F32) {
+        if (a.K.blk && !a.K.inv) {
+            static unsigned long long attr_b = 0;
+            set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
+            k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);
+            MR_LAUNCH_CHECK("k_xbdh");
+            return MR_SUCCESS;
+        }
+    }
+    static unsigned long long attr = 0;
+    set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
     k_xbdh<N, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
     MR_LAUNCH_CHECK("k_xbdh");
     return MR_SUCCESS;
