@@ -466,12 +466,139 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
     return MR_SUCCESS;
 }
 
+// Asynchronous 16-byte copies global -> shared (zero-filled past `bytes`).
+__device__ __forceinline__ void mr_cp_async16(void *sdst, const void *gsrc, unsigned bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mr_cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void mr_cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// `rows` rows of a tile of XT columns (row r at src + r * stride, nx valid
+// columns) into dst[r * XT + c], as 16-byte copies; columns past nx read 0.
+// src, stride and the tile start must be 16-byte aligned (even elements).
+template <int XT, int kNT>
+__device__ __forceinline__ void mr_cp_tile(float2 *dst, const float2 *src, int64_t stride,
+                                           int rows, int nx) {
+    constexpr int CPR = XT / 2;
+    for (int c = threadIdx.x; c < rows * CPR; c += kNT) {
+        const int r = c / CPR;
+        const int e0 = 2 * (c - r * CPR);
+        const int valid = nx - e0;
+        const unsigned bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
+        const float2 *g = bytes ? src + (int64_t)r * stride + e0 : src;
+        mr_cp_async16(dst + r * XT + e0, g, bytes);
+    }
+}
+
+// Inverse strided pass with the conj(S_c) coil sum (the last pass of 3-D /
+// stack plans), pipelined over the coils: while coil c is transformed, the
+// next coil's input tile and coil-map tile are already being copied into the
+// other half of a double buffer (cp.async), so the loads overlap the FFT
+// instead of stalling it. Same arithmetic and order as k_strided3<1, BUF,
+// COILSUM>. Shared memory: input and map tiles x 2 stages, FFT buffer, sum.
+template <int M, int XT, int kNT, int MINB>
+__global__ void __launch_bounds__(kNT, MINB) k_coilsum_pipe(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int TILE = M * XT;
+    float2 *wst = sm;                 // [2][M][XT] input tiles
+    float2 *sst = sm + 2 * TILE;      // [2][M][XT] coil-map tiles (n_out rows used)
+    float2 *buf = sm + 4 * TILE;      // FFT workspace
+    float2 *acc = sm + 5 * TILE;      // coil sum (n_out rows)
+    int64_t bid = blockIdx.x;
+    const int plane = (int)(bid % a.nplane);
+    bid /= a.nplane;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int64_t off0 = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
+    auto issue = [&](int cc, int st) {
+        const float2 *srcp = a.src + (int64_t)(cc * a.L + plane) * a.s_plane + off0;
+        mr_cp_tile<XT, kNT>(wst + st * TILE, srcp, a.s_axis, a.n_in, nx);
+        const float2 *sp = a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0;
+        mr_cp_tile<XT, kNT>(sst + st * TILE, sp, a.d_axis, a.n_out, nx);
+        mr_cp_async_commit();
+    };
+    issue(0, 0);
+    for (int cc = 0; cc < a.ncoil; ++cc) {
+        const int st = cc & 1;
+        if (cc + 1 < a.ncoil) {
+            issue(cc + 1, st ^ 1);
+            mr_cp_async_wait<1>();
+        } else {
+            mr_cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2 *w = wst + st * TILE;
+        const float2 *sv = sst + st * TILE;
+        auto load = [&](int b, int e) -> float2 {
+            int sa = e + a.shift_in;
+            if (sa >= M) sa -= M;
+            return sa < a.n_in ? w[sa * XT + b] : make_float2(0.f, 0.f);
+        };
+        auto store = [&](int b, int q, float2 v) {
+            int da = q + a.shift_out;
+            if (da >= M) da -= M;
+            if (da < a.n_out) {
+                const int ai = da * XT + b;
+                const float2 t = c_mulc(sv[ai], v);
+                acc[ai] = (cc == 0) ? t : c_add(acc[ai], t);
+            }
+        };
+        mrfix::fft_io<true, true, 1, M, XT, XT, 1, kNT>(buf, a.ax.tw, load, store);
+        __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < a.n_out * XT; idx += kNT) {
+        const int da = idx / XT;
+        const int xx = idx % XT;
+        if (xx < nx) {
+            float2 *o = a.dst + (int64_t)plane * a.d_plane + doff0 + (int64_t)da * a.d_axis + xx;
+            const float2 v = c_scale(acc[idx], a.scale);
+            *o = a.accumulate ? c_add(*o, v) : v;
+        }
+    }
+}
+
+// Whether the pipelined coil-sum pass can take these arguments: 16-byte
+// aligned tiles (even strides and offsets, aligned bases).
+inline bool mr_coilsum_pipe_ok(const mr_strided_args &a) {
+    return mr_env_int("MR_AHA_B200_NO_PIPE", 0) == 0 &&
+           (((uintptr_t)a.src | (uintptr_t)a.xs_s) & 15) == 0 &&
+           ((a.s_plane | a.s_axis | a.s_outer | a.img_plane | a.d_axis | a.d_outer) & 1) == 0 &&
+           a.ncoil >= 1;
+}
+
 template <int DIR, int LM, int SM, int M, int XT>
 int launch_s3(const mr_strided_args &a, cudaStream_t s) {
     constexpr int kNT = (M * XT > 10240) ? 512 : 256;
     // CTAs per SM the register budget must allow: small tiles need few
     // registers per thread, so more independent CTAs overlap their phases
     constexpr int MINB = (M * XT > 10240) ? 1 : (M * XT <= 2048 ? 4 : (M * XT <= 5120 ? 3 : 2));
+    if constexpr (SM == MR_SM_COILSUM && LM == MR_LM_BUF && DIR > 0 && XT % 2 == 0 &&
+                  mrfix::factor(M).n >= 2 && 6 * M * XT * 8 <= 112 * 1024) {
+        if (mr_coilsum_pipe_ok(a)) {
+            // CTAs per SM that the shared memory allows, at most 4
+            constexpr int PB = (6 * M * XT * 8 <= 48 * 1024) ? 4 : 2;
+            static unsigned long long attr_p = 0;
+            set_attr(k_coilsum_pipe<M, XT, 256, PB>, attr_p);
+            const int64_t nb = (int64_t)a.nxt * a.nouter * a.nplane;
+            if (nb <= 0) return MR_SUCCESS;
+            if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+            k_coilsum_pipe<M, XT, 256, PB><<<(unsigned)nb, 256,
+                                             (size_t)6 * M * XT * sizeof(float2), s>>>(a);
+            MR_LAUNCH_CHECK("k_coilsum_pipe");
+            return MR_SUCCESS;
+        }
+    }
     static unsigned long long attr = 0;
     set_attr(k_strided3<DIR, LM, SM, M, XT, kNT, MINB>, attr);
     size_t smem = (size_t)M * XT * sizeof(float2);

@@ -2,8 +2,10 @@
 oracle: half-length pass 3 for N in {64, 128, 192, 256} and every rank
 configuration (L = 4, 8 with several coils per tile, 16, and 32 with the
 split two-thread block multiply), strided passes of 256 / 384 / 512-point y
-lines and 16 / 32-point z lines; lower and upper packings, a coil count that
-does not fill the last tile, and a masked rank-32 kernel. Tolerance
+lines and 16 / 32-point z lines (the pipelined coil sum with a ragged last
+tile, and the plain one on an odd plane it cannot align); lower and upper
+packings, a coil count that does not fill the last tile, and a masked
+rank-32 kernel. Tolerance
 (relative L2): 1e-5."""
 
 import numpy as np
@@ -26,6 +28,8 @@ CASES = [
     ((256, 256, 2), 8, 2, "upper"),
     ((64, 64, 16), 4, 2, "lower"),
     ((64, 64, 32), 4, 2, "upper"),
+    ((30, 22, 16), 4, 3, "lower"),    # ragged last z tile (660 columns), pipelined coil sum
+    ((21, 25, 16), 2, 3, "upper"),    # odd plane (525 columns): unaligned, plain coil sum
 ]
 IDS = [f"{n[0]}x{n[1]}x{n[2]}-L{L}-C{c}-{t}" for n, L, c, t in CASES]
 
