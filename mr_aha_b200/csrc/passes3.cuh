@@ -568,6 +568,67 @@ __global__ void __launch_bounds__(kNT, MINB) k_coilsum_pipe(const __grid_constan
     }
 }
 
+// First pass of 3-D / stack plans (forward z lines of S_c x_l), pipelined
+// over the ranks: a CTA takes one coil's L planes of a tile; the coil-map
+// tile is copied once, and the next rank's image tile is copied (cp.async)
+// while the current one is transformed. Same arithmetic as k_strided3<-1,
+// XS, BUF> (S_c x_l, then the FFT), so the results are identical.
+template <int M, int XT, int kNT, int MINB>
+__global__ void __launch_bounds__(kNT, MINB) k_xs_pipe(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int TILE = M * XT;
+    float2 *sst = sm;                // coil-map tile (n_in rows)
+    float2 *xst = sm + TILE;         // [2] image tiles
+    float2 *buf = sm + 3 * TILE;     // FFT workspace
+    const int ncg = a.nplane / a.L;  // coils
+    int64_t bid = blockIdx.x;
+    const int cg = (int)(bid % ncg);
+    bid /= ncg;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int64_t off0 = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
+    mr_cp_tile<XT, kNT>(sst, a.xs_s + (int64_t)(a.coil0 + cg) * a.img_plane + off0, a.s_axis,
+                        a.n_in, nx);
+    mr_cp_tile<XT, kNT>(xst, a.xs_x + off0, a.s_axis, a.n_in, nx);
+    mr_cp_async_commit();
+    for (int l = 0; l < a.L; ++l) {
+        const int st = l & 1;
+        if (l + 1 < a.L) {
+            mr_cp_tile<XT, kNT>(xst + (st ^ 1) * TILE, a.xs_x + (int64_t)(l + 1) * a.img_plane + off0,
+                                a.s_axis, a.n_in, nx);
+            mr_cp_async_commit();
+            mr_cp_async_wait<1>();
+        } else {
+            mr_cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2 *xv = xst + st * TILE;
+        float2 *dstp = a.dst + (int64_t)(cg * a.L + l) * a.d_plane + doff0;
+        auto load = [&](int b, int e) -> float2 {
+            int sa = e + a.shift_in;
+            if (sa >= M) sa -= M;
+            return sa < a.n_in ? c_mul(sst[sa * XT + b], xv[sa * XT + b]) : make_float2(0.f, 0.f);
+        };
+        auto store = [&](int b, int q, float2 v) {
+            int da = q + a.shift_out;
+            if (da >= M) da -= M;
+            if (da < a.n_out && b < nx) dstp[(int64_t)da * a.d_axis + b] = c_scale(v, a.scale);
+        };
+        mrfix::fft_io<true, true, -1, M, XT, XT, 1, kNT>(buf, a.ax.tw, load, store);
+        __syncthreads();
+    }
+}
+
+inline bool mr_xs_pipe_ok(const mr_strided_args &a) {
+    return mr_env_int("MR_AHA_B200_NO_PIPE", 0) == 0 &&
+           (((uintptr_t)a.xs_x | (uintptr_t)a.xs_s) & 15) == 0 &&
+           ((a.s_axis | a.s_outer | a.img_plane) & 1) == 0 && a.L >= 1 &&
+           a.nplane % a.L == 0;
+}
+
 // Whether the pipelined coil-sum pass can take these arguments: 16-byte
 // aligned tiles (even strides and offsets, aligned bases).
 inline bool mr_coilsum_pipe_ok(const mr_strided_args &a) {
@@ -583,6 +644,21 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
     // CTAs per SM the register budget must allow: small tiles need few
     // registers per thread, so more independent CTAs overlap their phases
     constexpr int MINB = (M * XT > 10240) ? 1 : (M * XT <= 2048 ? 4 : (M * XT <= 5120 ? 3 : 2));
+    if constexpr (SM == MR_SM_BUF && LM == MR_LM_XS && DIR < 0 && XT % 2 == 0 &&
+                  mrfix::factor(M).n >= 2 && 4 * M * XT * 8 <= 112 * 1024) {
+        if (mr_xs_pipe_ok(a)) {
+            constexpr int PB = (4 * M * XT * 8 <= 48 * 1024) ? 4 : 2;
+            static unsigned long long attr_x = 0;
+            set_attr(k_xs_pipe<M, XT, 256, PB>, attr_x);
+            const int64_t nb = (int64_t)a.nxt * a.nouter * (a.nplane / a.L);
+            if (nb <= 0) return MR_SUCCESS;
+            if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+            k_xs_pipe<M, XT, 256, PB><<<(unsigned)nb, 256, (size_t)4 * M * XT * sizeof(float2),
+                                        s>>>(a);
+            MR_LAUNCH_CHECK("k_xs_pipe");
+            return MR_SUCCESS;
+        }
+    }
     if constexpr (SM == MR_SM_COILSUM && LM == MR_LM_BUF && DIR > 0 && XT % 2 == 0 &&
                   mrfix::factor(M).n >= 2 && 6 * M * XT * 8 <= 112 * 1024) {
         if (mr_coilsum_pipe_ok(a)) {
