@@ -368,6 +368,38 @@ void set_attr(F *f, unsigned long long &mask) {
     }
 }
 
+// Asynchronous 16-byte copies global -> shared (zero-filled past `bytes`).
+__device__ __forceinline__ void mr_cp_async16(void *sdst, const void *gsrc, unsigned bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mr_cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void mr_cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// `rows` rows of a tile of XT columns (row r at src + r * stride, nx valid
+// columns) into dst[r * XT + c], as 16-byte copies; columns past nx read 0.
+// src, stride and the tile start must be 16-byte aligned (even elements).
+template <int XT, int kNT>
+__device__ __forceinline__ void mr_cp_tile(float2 *dst, const float2 *src, int64_t stride,
+                                           int rows, int nx) {
+    constexpr int CPR = XT / 2;
+    for (int c = threadIdx.x; c < rows * CPR; c += kNT) {
+        const int r = c / CPR;
+        const int e0 = 2 * (c - r * CPR);
+        const int valid = nx - e0;
+        const unsigned bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
+        const float2 *g = bytes ? src + (int64_t)r * stride + e0 : src;
+        mr_cp_async16(dst + r * XT + e0, g, bytes);
+    }
+}
+
 // Strided passes of length M = 2N whose input (forward) or output (inverse)
 // is the N image rows, without the zero half: the forward pass computes the
 // ramp-free spectrum X'[k] = sum_n x[n] W_M^{kn} as X'[2m] = FFT_N(x)[m],
@@ -445,6 +477,61 @@ __global__ void __launch_bounds__(kNT, MINB) k_strided_hi(const __grid_constant_
     }
 }
 
+// The half-length forward y pass pipelined over planes: a CTA takes PG
+// planes of one (x tile, z) position; the next plane's rows are copied
+// (cp.async) into the other stage while the current plane is transformed.
+// The first FFT pass reads the stage (the odd line times t[n]), the last one
+// writes the spectrum rows. Same arithmetic as k_strided_hf.
+template <int N, int XT, int kNT, int MINB, int PG>
+__global__ void __launch_bounds__(kNT, MINB) k_hf_pipe(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int NL = 2 * XT;
+    constexpr int STG = N * XT;
+    float2 *stg = sm;               // [2][N][XT]
+    float2 *buf = sm + 2 * STG;     // [N][2 XT]
+    const int ngrp = (a.nplane + PG - 1) / PG;
+    int64_t bid = blockIdx.x;
+    const int grp = (int)(bid % ngrp);
+    bid /= ngrp;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int p0 = grp * PG;
+    const int np = min(PG, a.nplane - p0);
+    const int64_t soff = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff = (int64_t)outer * a.d_outer + x0;
+    const float2 *tw = a.ax.tw;
+    mr_cp_tile<XT, kNT>(stg, a.src + (int64_t)p0 * a.s_plane + soff, a.s_axis, N, nx);
+    mr_cp_async_commit();
+    for (int i = 0; i < np; ++i) {
+        const int st = i & 1;
+        if (i + 1 < np) {
+            mr_cp_tile<XT, kNT>(stg + (st ^ 1) * STG, a.src + (int64_t)(p0 + i + 1) * a.s_plane + soff,
+                                a.s_axis, N, nx);
+            mr_cp_async_commit();
+            mr_cp_async_wait<1>();
+        } else {
+            mr_cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2 *sv = stg + st * STG;
+        float2 *dstp = a.dst + (int64_t)(p0 + i) * a.d_plane + doff;
+        auto load = [&](int bl, int e) -> float2 {
+            const int b = bl % XT;
+            const float2 v = sv[e * XT + b];
+            return bl >= XT ? c_mul(v, __ldg(tw + e)) : v;
+        };
+        auto store = [&](int bl, int q, float2 v) {
+            const int b = bl % XT;
+            const int k = 2 * q + (bl >= XT ? 1 : 0);
+            if (b < nx) dstp[(int64_t)k * a.d_axis + b] = c_scale(v, a.scale);
+        };
+        mrfix::fft_io<true, true, -1, N, NL, NL, 1, kNT, 2>(buf, tw, load, store);
+        __syncthreads();
+    }
+}
+
 template <int DIR, int N, int XT>
 int launch_sh(const mr_strided_args &a, cudaStream_t s) {
     constexpr int T = 2 * N * XT;
@@ -455,6 +542,19 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
     const int64_t nblk = (int64_t)a.nxt * a.nouter * a.nplane;
     if (nblk <= 0) return MR_SUCCESS;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+    if constexpr (DIR < 0 && XT % 2 == 0 && 4 * N * XT * 8 <= 112 * 1024) {
+        constexpr int PG = 8;
+        if (mr_env_int("MR_AHA_B200_NO_PIPE", 0) == 0 && (((uintptr_t)a.src) & 15) == 0 &&
+            ((a.s_plane | a.s_axis | a.s_outer) & 1) == 0) {
+            static unsigned long long attr_p = 0;
+            set_attr(k_hf_pipe<N, XT, kNT, 2, PG>, attr_p);
+            const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
+            k_hf_pipe<N, XT, kNT, 2, PG><<<(unsigned)nb, kNT, (size_t)4 * N * XT * sizeof(float2),
+                                           s>>>(a);
+            MR_LAUNCH_CHECK("k_hf_pipe");
+            return MR_SUCCESS;
+        }
+    }
     if constexpr (DIR < 0) {
         set_attr(k_strided_hf<N, XT, kNT, MINB>, attr);
         k_strided_hf<N, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
@@ -464,38 +564,6 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
     }
     MR_LAUNCH_CHECK("k_strided_h");
     return MR_SUCCESS;
-}
-
-// Asynchronous 16-byte copies global -> shared (zero-filled past `bytes`).
-__device__ __forceinline__ void mr_cp_async16(void *sdst, const void *gsrc, unsigned bytes) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ void mr_cp_async_commit() {
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void mr_cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// `rows` rows of a tile of XT columns (row r at src + r * stride, nx valid
-// columns) into dst[r * XT + c], as 16-byte copies; columns past nx read 0.
-// src, stride and the tile start must be 16-byte aligned (even elements).
-template <int XT, int kNT>
-__device__ __forceinline__ void mr_cp_tile(float2 *dst, const float2 *src, int64_t stride,
-                                           int rows, int nx) {
-    constexpr int CPR = XT / 2;
-    for (int c = threadIdx.x; c < rows * CPR; c += kNT) {
-        const int r = c / CPR;
-        const int e0 = 2 * (c - r * CPR);
-        const int valid = nx - e0;
-        const unsigned bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
-        const float2 *g = bytes ? src + (int64_t)r * stride + e0 : src;
-        mr_cp_async16(dst + r * XT + e0, g, bytes);
-    }
 }
 
 // Inverse strided pass with the conj(S_c) coil sum (the last pass of 3-D /
