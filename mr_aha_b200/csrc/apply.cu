@@ -107,7 +107,8 @@ static void plan_pick_v2(mr_aha_plan p, size_t lim) {
         // measured at 320 x 320 x 56, L = 16, 12 coils: forward 8.2 ms with
         // 8-column tiles (8.8 with 16), inverse 6.6 ms with 16 (7.2 with 8)
         p->yh_f = mr_half_strided_xt(g.n[1], wy ? wy : 8);
-        p->yh_i = p->yh_f > 0 ? mr_half_strided_xt(g.n[1], wy ? wy : 16) : 0;
+        const int wyi = mr_env_int("MR_AHA_B200_XT_YI", 0);  // inverse only (tuning)
+        p->yh_i = p->yh_f > 0 ? mr_half_strided_xt(g.n[1], wyi ? wyi : (wy ? wy : 16)) : 0;
         if (p->yh_i == 0) p->yh_f = 0;
     }
 }

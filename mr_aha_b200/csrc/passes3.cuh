@@ -532,6 +532,65 @@ __global__ void __launch_bounds__(kNT, MINB) k_hf_pipe(const __grid_constant__ m
     }
 }
 
+// The half-length inverse y pass pipelined over planes (as k_hf_pipe): the
+// next plane's 2N spectrum rows are copied into the other stage while the
+// current plane is transformed; the first FFT pass reads the stage (row
+// 2e + p for element e of line parity p), the combine loop writes the N
+// image rows. Same arithmetic as k_strided_hi.
+template <int N, int XT, int kNT, int MINB, int PG>
+__global__ void __launch_bounds__(kNT, MINB) k_hi_pipe(const __grid_constant__ mr_strided_args a) {
+    extern __shared__ float2 sm[];
+    constexpr int NL = 2 * XT;
+    constexpr int STG = 2 * N * XT;
+    float2 *stg = sm;               // [2][2N][XT]
+    float2 *buf = sm + 2 * STG;     // [N][2 XT]
+    const int ngrp = (a.nplane + PG - 1) / PG;
+    int64_t bid = blockIdx.x;
+    const int grp = (int)(bid % ngrp);
+    bid /= ngrp;
+    const int xtile = (int)(bid % a.nxt);
+    const int outer = (int)(bid / a.nxt);
+    const int x0 = xtile * XT;
+    const int nx = min(XT, a.nfast - x0);
+    const int p0 = grp * PG;
+    const int np = min(PG, a.nplane - p0);
+    const int64_t soff = (int64_t)outer * a.s_outer + x0;
+    const int64_t doff = (int64_t)outer * a.d_outer + x0;
+    const float2 *tw = a.ax.tw;
+    mr_cp_tile<XT, kNT>(stg, a.src + (int64_t)p0 * a.s_plane + soff, a.s_axis, 2 * N, nx);
+    mr_cp_async_commit();
+    for (int i = 0; i < np; ++i) {
+        const int st = i & 1;
+        if (i + 1 < np) {
+            mr_cp_tile<XT, kNT>(stg + (st ^ 1) * STG, a.src + (int64_t)(p0 + i + 1) * a.s_plane + soff,
+                                a.s_axis, 2 * N, nx);
+            mr_cp_async_commit();
+            mr_cp_async_wait<1>();
+        } else {
+            mr_cp_async_wait<0>();
+        }
+        __syncthreads();
+        const float2 *sv = stg + st * STG;
+        auto load = [&](int bl, int e) -> float2 {
+            const int b = bl % XT;
+            return sv[(2 * e + (bl >= XT ? 1 : 0)) * XT + b];
+        };
+        mrfix::fft_io<true, false, 1, N, NL, NL, 1, kNT, 2>(buf, tw, load, mrfix::no_store());
+        float2 *dstp = a.dst + (int64_t)(p0 + i) * a.d_plane + doff;
+        for (int idx = threadIdx.x; idx < N * XT; idx += kNT) {
+            const int n = idx / XT;
+            const int b = idx - n * XT;
+            if (b < nx) {
+                const float2 e = buf[n * NL + b];
+                const float2 o = buf[n * NL + XT + b];
+                dstp[(int64_t)n * a.d_axis + b] =
+                    c_scale(c_add(e, c_mulc(__ldg(tw + n), o)), a.scale);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <int DIR, int N, int XT>
 int launch_sh(const mr_strided_args &a, cudaStream_t s) {
     constexpr int T = 2 * N * XT;
@@ -552,6 +611,19 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
             k_hf_pipe<N, XT, kNT, 2, PG><<<(unsigned)nb, kNT, (size_t)4 * N * XT * sizeof(float2),
                                            s>>>(a);
             MR_LAUNCH_CHECK("k_hf_pipe");
+            return MR_SUCCESS;
+        }
+    }
+    if constexpr (DIR > 0 && XT % 2 == 0 && 6 * N * XT * 8 <= 64 * 1024) {
+        constexpr int PG = 8;
+        if (mr_env_int("MR_AHA_B200_NO_PIPE", 0) == 0 && (((uintptr_t)a.src) & 15) == 0 &&
+            ((a.s_plane | a.s_axis | a.s_outer) & 1) == 0) {
+            static unsigned long long attr_p = 0;
+            set_attr(k_hi_pipe<N, XT, kNT, 3, PG>, attr_p);
+            const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
+            k_hi_pipe<N, XT, kNT, 3, PG><<<(unsigned)nb, kNT, (size_t)6 * N * XT * sizeof(float2),
+                                           s>>>(a);
+            MR_LAUNCH_CHECK("k_hi_pipe");
             return MR_SUCCESS;
         }
     }
@@ -815,7 +887,7 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
 #define MR_XH_LIST(X) MR_XH_LIST_A(X) MR_XH_LIST_B(X) MR_XH_LIST_C(X)
 
 // Half-length strided passes (N, tile width), in p3_yhalf.cu.
-#define MR_SH_LIST(X) X(320, 16) X(320, 8) X(256, 16) X(256, 8) X(192, 16) X(192, 8) \
+#define MR_SH_LIST(X) X(320, 16) X(320, 8) X(320, 4) X(256, 16) X(256, 8) X(192, 16) X(192, 8) \
     X(128, 16) X(128, 32) X(64, 32) X(64, 16)
 
 // Dispatchers of the other translation units: launch when (M, tile) /
