@@ -195,6 +195,7 @@ PROTOTYPES = {
                                             ctypes.c_int, ctypes.POINTER(_P)]),
     "mr_b200_batch_execute": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
     "mr_b200_batch_destroy": (ctypes.c_int, [_P]),
+    "mr_b200_op_blocked_copy": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_op_device_bytes": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64)]),
     "mr_b200_cg_busy": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_cg_iterations": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),

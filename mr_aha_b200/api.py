@@ -528,6 +528,16 @@ class AhAOp:
               "mr_b200_op_autotune")
         return float(ms.value)
 
+    def blocked_copy(self, enable: bool) -> bool:
+        """Free (False) or build (True, if it fits) the blocked complex64
+        kernel copy read by pass 3 (``mr_b200_op_blocked_copy``); returns
+        whether a copy exists."""
+        self._check_open()
+        built = ctypes.c_int(0)
+        check(lib.mr_b200_op_blocked_copy(self._handle, 1 if enable else 0, ctypes.byref(built)),
+              "mr_b200_op_blocked_copy")
+        return bool(built.value)
+
     @property
     def device_bytes(self) -> int:
         """Device memory held by the operator (``mr_b200_op_device_bytes``)."""

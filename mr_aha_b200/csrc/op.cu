@@ -430,6 +430,7 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
             mr_set_error("the complex64 kernel was released; it cannot be restored");
         } else {
             op->kf = MR_KF_F32;
+            op_build_blocked(op);
         }
     } else if (!op->K) {
         rc = MR_ERR_UNSUPPORTED;
@@ -437,6 +438,10 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
     } else {
         const int64_t nloc = op->cfg.is_masked ? op->cfg.num_masked : mr_pad_size(&op->cfg);
         const int64_t ntri = mr_num_tri(op->cfg.L);
+        // the blocked complex64 copy serves only the complex64 format: give
+        // its memory back before the 16-bit copy is allocated
+        if (op->K_blk) cudaFree(op->K_blk);
+        op->K_blk = nullptr;
         if (op->K16) cudaFree(op->K16);
         if (op->K16_scale) cudaFree(op->K16_scale);
         op->K16 = nullptr;
@@ -552,6 +557,24 @@ extern "C" int mr_b200_op_autotune(mr_op op, int reps, float *ms) {
     }
     if (prev != op->dev) cudaSetDevice(prev);
     return rc;
+}
+
+extern "C" int mr_b200_op_blocked_copy(mr_op op, int enable, int *built) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_blocked_copy: op is NULL");
+    int prev = 0;
+    MR_CUDA_TRY(cudaGetDevice(&prev));
+    if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
+    if (enable) {
+        if (op->kf == MR_KF_F32) op_build_blocked(op);
+    } else if (op->K_blk) {
+        cudaStreamSynchronize(op->stream);
+        cudaFree(op->K_blk);
+        op->K_blk = nullptr;
+    }
+    if (prev != op->dev) cudaSetDevice(prev);
+    if (built) *built = op->K_blk != nullptr;
+    return MR_SUCCESS;
 }
 
 extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {

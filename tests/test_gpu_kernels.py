@@ -87,6 +87,12 @@ def test_blocked_kernel_copy_equals_reference_layout(n_dim, L, nc, monkeypatch):
             ys.append(host(op(dev(p["x"]))))
             devbytes.append(op.device_bytes)
             K = host(op.kernel())
+            if off == "0":
+                # freeing the copy switches pass 3 to the reference layout
+                assert op.blocked_copy(False) is False
+                assert op.device_bytes < devbytes[0]
+                assert np.array_equal(host(op(dev(p["x"]))), ys[0])
+                assert op.blocked_copy(True) is True
     assert devbytes[0] > devbytes[1]          # the copy was built
     assert np.array_equal(ys[0], ys[1])
     ref = O.aha_toeplitz("stack", n_dim, synth.default_phi2_dim("stack", n_dim), L, p["x"],
