@@ -193,3 +193,29 @@ def test_synthetic_workloads_are_seeded():
     np.testing.assert_allclose(s, 1.0, rtol=1e-5)
     Phi = a["Phi"]
     np.testing.assert_allclose(Phi @ Phi.conj().T, np.eye(Phi.shape[0]), atol=1e-12)
+
+
+def test_added_entry_points_reject_null_arguments():
+    """The solver, batch and operator-extension entry points check their
+    arguments before any device work: NULL handles give MR_ERR_INVALID_ARG
+    (-1) with a message, destroy(NULL) is a no-op (as mr_op_destroy)."""
+    lib = _lib()
+    h = ctypes.c_void_p(1)
+    assert lib.mr_b200_cg_create(None, None, None, 0.0, 0, 10, ctypes.byref(h)) == -1
+    assert h.value is None and b"op is NULL" in lib.mr_last_error()
+    assert lib.mr_b200_cg_step(None, 1) == -1
+    n = ctypes.c_int(0)
+    rr = (ctypes.c_double * 2)()
+    assert lib.mr_b200_cg_residuals(None, rr, 2, ctypes.byref(n)) == -1
+    assert lib.mr_b200_cg_busy(None, ctypes.byref(n)) == -1
+    assert lib.mr_b200_cg_iterations(None, ctypes.byref(n)) == -1
+    assert lib.mr_b200_cg_destroy(None) == 0
+    h = ctypes.c_void_p(1)
+    assert lib.mr_b200_batch_create(None, 0, 4, 0, ctypes.byref(h)) == -1
+    assert h.value is None and b"no operators" in lib.mr_last_error()
+    assert lib.mr_b200_batch_execute(None, None, None, None) == -1
+    assert lib.mr_b200_batch_destroy(None) == 0
+    assert lib.mr_b200_op_blocked_copy(None, 0, None) == -1
+    assert lib.mr_b200_op_autotune(None, 1, None) == -1
+    b = ctypes.c_uint64(0)
+    assert lib.mr_b200_op_device_bytes(None, ctypes.byref(b)) == -1
