@@ -68,6 +68,19 @@ MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
  * Synchronous. */
 MR_EXPORT int mr_b200_op_autotune(mr_op op, int reps, float *ms);
 
+/* No reference counterpart. Launch trace of the calling host thread:
+ * enable = 1 clears the trace and records, for every kernel the library
+ * launches from this thread afterwards, one line naming it (the specialised
+ * kernels with their template arguments, e.g.
+ * "k_xbdh<N=320,L=16,NC=1,F32,256,blocked>"); enable = 0 stops recording.
+ * For tests and tuning: it shows which instantiation ran each pass. */
+MR_EXPORT int mr_b200_trace_launches(int enable);
+
+/* No reference counterpart. Copies the calling thread's trace into buf
+ * (NUL-terminated, truncated to cap - 1 bytes; buf may be NULL) and returns
+ * its full length in bytes. */
+MR_EXPORT int64_t mr_b200_trace_read(char *buf, size_t cap);
+
 /* Size of the library's static device scratch array used by
  * mr_b200_aha_toeplitz_noalloc (reserved on every GPU that loads the
  * library, until the process exits). */

@@ -1,27 +1,24 @@
-"""Array-level interface, a drop-in for the reference's ``python/mr_aha/api.py``.
+"""Array-level interface of the library: the functions, argument meanings,
+shapes and exceptions of the reference's Python binding
+(``python/mr_aha/api.py``: ``make_config`` ``:211-324``, ``calc_mask``
+``:393-447``, ``calc_toep`` ``:556-639``, ``aha_toeplitz`` ``:642-701``,
+``AhAOp`` / ``create_op`` ``:745-1255``), implemented over this package's C
+ABI.
 
-Same functions, argument meanings, shapes and errors as the reference binding
-(``make_config`` ``api.py:211-324``, ``calc_mask`` ``:393-447``,
-``calc_toep`` ``:556-639``, ``aha_toeplitz`` ``:642-701``, ``AhAOp`` /
-``create_op`` ``:745-1255``). Arrays are CUDA device arrays: a
-``torch.Tensor`` on a CUDA device, or any object exposing
-``__cuda_array_interface__`` (CuPy, Numba, ...). Shapes are row-major, i.e.
-the column-major shapes of the C API reversed:
+Arrays live on the GPU: a CUDA ``torch.Tensor``, or any object exposing
+``__cuda_array_interface__``. Every array is C-contiguous; data arrays are
+``complex64``, ``traj`` is ``float32`` and ``mask`` ``int64``. Axis order is
+row-major, so each shape reads right to left against the C header's
+column-major one: an image ``x`` is ``(L, Nz, Ny, Nx)``, coil maps ``SEs``
+``(C, Nz, Ny, Nx)``, the kernel ``phi2_toep`` ``(ntri, Mz, My, Mx)`` (or
+``(ntri, num_masked)``), Gram blocks ``phi2`` ``(L, L, Nkz, Ntrajs)`` for a
+stack (``(L, L, Ntrajs)`` otherwise) and the trajectory ``traj``
+``(ndim, Nkx, Ntrajs)``; 2-D configurations drop the z axis.
 
-============================  =======================================
-column-major (C API)          row-major (this module)
-============================  =======================================
-``x[Nx, Ny, Nz, L]``          ``x[L, Nz, Ny, Nx]``
-``SEs[Nx, Ny, Nz, Nc]``       ``SEs[Nc, Nz, Ny, Nx]``
-``phi2_toep[Mx, My, Mz, T]``  ``phi2_toep[T, Mz, My, Mx]``
-``phi2[Ntrajs, Nkz, L, L]``   ``phi2[L, L, Nkz, Ntrajs]`` (stack)
-``traj[Ntrajs, Nkx, ndim]``   ``traj[ndim, Nkx, Ntrajs]``
-============================  =======================================
-
-``complex64`` for the data arrays, ``float32`` for ``traj``, ``int64`` for
-``mask``; every array C-contiguous. The Gram blocks multiply the rank row
-vector from the right, ``v <- v Phi2`` (``include/mr_aha/mr_aha.h:33-62`` of
-the reference).
+Every size is checked against the C library's own size helpers
+(``mr_x_size``, ``mr_se_size``, ``mr_phi2_toep_size``) by one routine,
+:func:`_validate`, before any pointer crosses the ABI. Gram blocks act on the
+rank row vector from the right (``v <- v B``), the reference's convention.
 """
 
 from __future__ import annotations
@@ -161,52 +158,56 @@ def _stream_ptr(stream):
     raise TypeError("stream must be None, an int handle, a torch.cuda.Stream or expose .ptr")
 
 
+def _grid_dims(traj_type: int, n_dim, phi2_dim) -> tuple:
+    """Column-major image and grid extents of a configuration. The grid
+    defaults to twice the image along every transformed axis; a stack keeps
+    its z extent (its kz axis is not oversampled)."""
+    n_spatial = 2 if traj_type == TrajType.TWO_D else 3
+    n = tuple(int(v) for v in n_dim)
+    if len(n) != n_spatial:
+        raise ValueError(f"n_dim must have {n_spatial} entries for this trajectory type, "
+                         f"got {len(n)}")
+    if phi2_dim is None:
+        m = tuple(v if (traj_type == TrajType.STACK and ax == 2) else 2 * v
+                  for ax, v in enumerate(n))
+    else:
+        m = tuple(int(v) for v in phi2_dim)
+    if len(m) != n_spatial:
+        raise ValueError(f"phi2_dim must have {n_spatial} entries, got {len(m)}")
+    return n, m
+
+
 def make_config(traj_type, n_dim: Sequence[int], L: int, *,
                 phi2_dim: Optional[Sequence[int]] = None, triangulation="lower",
                 is_masked: bool = False, num_masked: int = 0, n_coils: int = 1,
                 eps: float = 1e-6, gpu_device_id: int = -1, stream=None,
                 mem_fraction: float = 0.5, verbose: bool = False,
                 mask_radius: int = DEFAULT_MASK_RADIUS) -> MRConfig:
-    """Build a validated :class:`MRConfig` (reference ``api.py:211-324``).
+    """A validated :class:`MRConfig` (the reference's ``make_config``).
 
-    ``n_dim`` / ``phi2_dim`` are column-major ``(Nx, Ny[, Nz])``;
-    ``phi2_dim`` defaults to ``2 * n_dim`` except ``Mz = Nz`` for a stack.
-    ``is_masked=True`` with ``num_masked=0`` is accepted (filled in later).
+    ``n_dim`` / ``phi2_dim`` are column-major ``(Nx, Ny[, Nz])``. A masked
+    configuration may leave ``num_masked`` at 0: the count is taken from the
+    mask when the configuration is first used with one.
     """
     tt = TrajType.parse(traj_type)
+    n, m = _grid_dims(tt, n_dim, phi2_dim)
     cfg = MRConfig()
     check(lib.mr_config_defaults(ctypes.byref(cfg), tt), "mr_config_defaults")
-    n_spatial = cfg.n_spatial
-    n_dim = [int(v) for v in n_dim]
-    if len(n_dim) != n_spatial:
-        raise ValueError(f"n_dim must have {n_spatial} entries for this trajectory type, "
-                         f"got {len(n_dim)}")
-    if phi2_dim is None:
-        phi2_dim = [2 * v for v in n_dim]
-        if tt == TrajType.STACK:
-            phi2_dim[2] = n_dim[2]
-    else:
-        phi2_dim = [int(v) for v in phi2_dim]
-    if len(phi2_dim) != n_spatial:
-        raise ValueError(f"phi2_dim must have {n_spatial} entries, got {len(phi2_dim)}")
-    for i in range(n_spatial):
-        cfg.n_dim[i] = n_dim[i]
-        cfg.phi2_dim[i] = phi2_dim[i]
-    cfg.L = int(L)
-    cfg.triangulation = Triangulation.parse(triangulation)
-    cfg.is_masked = 1 if is_masked else 0
-    cfg.num_masked = int(num_masked)
-    cfg.n_coils = int(n_coils)
-    cfg.eps = float(eps)
-    cfg.gpu_device_id = int(gpu_device_id)
-    cfg.mem_fraction = float(mem_fraction)
-    cfg.verbose = 1 if verbose else 0
-    cfg.mask_radius = int(mask_radius)
-    cfg.stream = _stream_ptr(stream)
-    probe = MRConfig.from_buffer_copy(cfg)
-    if probe.is_masked and probe.num_masked == 0:
-        probe.is_masked = 0
-    check(lib.mr_config_validate(ctypes.byref(probe)), "mr_config_validate")
+    cfg.n_dim[:len(n)] = n
+    cfg.phi2_dim[:len(m)] = m
+    scalars = dict(L=int(L), triangulation=Triangulation.parse(triangulation),
+                   is_masked=int(bool(is_masked)), num_masked=int(num_masked),
+                   n_coils=int(n_coils), eps=float(eps), gpu_device_id=int(gpu_device_id),
+                   mem_fraction=float(mem_fraction), verbose=int(bool(verbose)),
+                   mask_radius=int(mask_radius), stream=_stream_ptr(stream))
+    for field, value in scalars.items():
+        setattr(cfg, field, value)
+    # validate with a stand-in count of one masked location when the count
+    # is still open; the real count is checked once a mask is supplied
+    trial = MRConfig.from_buffer_copy(cfg)
+    if trial.is_masked and trial.num_masked == 0:
+        trial.num_masked = 1
+    check(lib.mr_config_validate(ctypes.byref(trial)), "mr_config_validate")
     return cfg
 
 
@@ -228,13 +229,58 @@ def _image_shape(cfg: MRConfig) -> tuple:
 
 
 def _check_traj(cfg: MRConfig, traj):
+    """``(Ntrajs, Nkx)`` of a trajectory shaped ``(ndim, Nkx, Ntrajs)``."""
     ndim_traj = 3 if cfg.traj_type == TrajType.THREE_D else 2
-    shape = tuple(traj.shape) if _is_torch(traj) else tuple(traj.__cuda_array_interface__["shape"])
+    shape = _shape(traj)
     if len(shape) != 3 or shape[0] != ndim_traj:
         raise ValueError(f"traj must be shaped (ndim, Nkx, Ntrajs) with ndim = {ndim_traj}, "
                          f"got {shape}")
-    _, Nkx, Ntrajs = shape
-    return int(Ntrajs), int(Nkx)
+    return int(shape[2]), int(shape[1])
+
+
+def _gram_size(cfg: MRConfig, n_traj: int) -> int:
+    """Elements of ``phi2``: one ``L x L`` block per readout (and per kz
+    plane of a stack)."""
+    n_kz = cfg.phi2_dim[2] if cfg.traj_type == TrajType.STACK else 1
+    return cfg.L * cfg.L * n_kz * n_traj
+
+
+_SIZE_OF = {"x": "mr_x_size", "out": "mr_x_size", "SEs": "mr_se_size",
+            "phi2_toep": "mr_phi2_toep_size"}
+
+
+def _validate(cfg: MRConfig, need_mask: bool = True, **arrays) -> tuple:
+    """Check the arrays of one call against the configuration's contract.
+
+    Image-, map- and kernel-sized arrays (``x``, ``out``, ``SEs``,
+    ``phi2_toep``) must hold exactly the element count the C library's size
+    helper gives for ``cfg``; ``phi2`` must match ``traj``'s readouts. A
+    masked configuration needs a mask (when ``need_mask``) whose length is
+    ``cfg.num_masked``, or sets that count when the configuration left it at
+    0 (then ``cfg`` is validated again). Arrays passed as None are skipped.
+    Returns ``(Ntrajs, Nkx)`` of ``traj`` (``(0, 0)`` without one). Raises
+    ``ValueError`` for a size or mask mismatch."""
+    traj = arrays.pop("traj", None)
+    phi2 = arrays.pop("phi2", None)
+    mask = arrays.pop("mask", None)
+    n_traj, n_kx = _check_traj(cfg, traj) if traj is not None else (0, 0)
+    if phi2 is not None:
+        _check_size(phi2, _gram_size(cfg, n_traj), "phi2")
+    if cfg.is_masked and (mask is not None or need_mask):
+        if mask is None:
+            raise ValueError("cfg.is_masked is set, so a mask is required")
+        n_masked = _size(mask)
+        if cfg.num_masked == 0:
+            cfg.num_masked = n_masked
+            check(lib.mr_config_validate(ctypes.byref(cfg)), "mr_config_validate")
+        elif n_masked != int(cfg.num_masked):
+            raise ValueError(f"mask has {n_masked} elements but cfg.num_masked is "
+                             f"{cfg.num_masked}")
+    for name, array in arrays.items():
+        if array is not None:
+            helper = getattr(lib, _SIZE_OF[name.lstrip("_")])
+            _check_size(array, int(helper(ctypes.byref(cfg))), name)
+    return n_traj, n_kx
 
 
 def calc_mask(cfg: MRConfig, traj, *, radius: Optional[int] = None):
@@ -254,40 +300,22 @@ def calc_mask(cfg: MRConfig, traj, *, radius: Optional[int] = None):
     return mask
 
 
-def _check_gram(cfg: MRConfig, phi2, traj, mask):
-    Ntrajs, Nkx = _check_traj(cfg, traj)
-    nkz = cfg.phi2_dim[2] if cfg.traj_type == TrajType.STACK else 1
-    _check_size(phi2, cfg.L * cfg.L * nkz * Ntrajs, "phi2")
-    if cfg.is_masked:
-        if mask is None:
-            raise ValueError("cfg.is_masked is set, so a mask is required")
-        if cfg.num_masked == 0:
-            cfg.num_masked = _size(mask)
-            check(lib.mr_config_validate(ctypes.byref(cfg)), "mr_config_validate")
-        elif _size(mask) != int(cfg.num_masked):
-            raise ValueError(f"mask has {_size(mask)} elements but cfg.num_masked is "
-                             f"{cfg.num_masked}")
-    return Ntrajs, Nkx
-
-
 def calc_toep(cfg: MRConfig, phi2, traj, mask=None, out=None, nufft: Optional[str] = None):
-    """Toeplitz kernel ``phi2_toep`` from the Gram blocks (reference ``api.py:556-639``).
+    """The Toeplitz kernel ``phi2_toep`` of the Gram blocks ``phi2`` sampled
+    at ``traj`` (the reference's ``calc_toep``), built on the GPU.
 
-    ``nufft`` is accepted for signature compatibility; only ``None`` /
-    ``'library'`` (the on-GPU build) exist in this implementation.
+    ``nufft`` exists for signature compatibility: the library's own build is
+    the only one (``None`` or ``'library'``).
     """
     if nufft not in (None, "library"):
         raise ValueError(f"nufft={nufft!r}: only the library build is available")
-    Ntrajs, Nkx = _check_gram(cfg, phi2, traj, mask)
-    shape = phi2_toep_shape(cfg)
-    expected = int(lib.mr_phi2_toep_size(ctypes.byref(cfg)))
+    n_traj, n_kx = _validate(cfg, traj=traj, phi2=phi2, mask=mask)
     if out is None:
-        out = _empty(shape, "complex64", _device_of(phi2, traj))
-    else:
-        _check_size(out, expected, "out")
+        out = _empty(phi2_toep_shape(cfg), "complex64", _device_of(phi2, traj))
+    _validate(cfg, need_mask=False, phi2_toep=out)
     check(lib.mr_calc_toep(ctypes.byref(cfg), _ptr(phi2, "phi2", "complex64"),
-                           _ptr(traj, "traj", "float32"), ctypes.c_int64(Ntrajs),
-                           ctypes.c_int64(Nkx), _ptr(mask, "mask", "int64", allow_none=True),
+                           _ptr(traj, "traj", "float32"), ctypes.c_int64(n_traj),
+                           ctypes.c_int64(n_kx), _ptr(mask, "mask", "int64", allow_none=True),
                            _ptr(out, "out", "complex64")), "mr_calc_toep")
     return out
 
@@ -306,22 +334,20 @@ def calc_toep_from_psf(cfg: MRConfig, psf, t0: int, out, mask=None):
     return out
 
 
+def _out_like(x, out):
+    """``out``, or a new complex64 array shaped like ``x`` on its device."""
+    return _empty(_shape(x), "complex64", _device_of(x)) if out is None else out
+
+
 def aha_toeplitz(cfg: MRConfig, x, SEs, phi2_toep, mask=None, out=None):
-    """One-shot Toeplitz ``A^H A x`` (reference ``api.py:642-701``)."""
-    _check_size(x, int(lib.mr_x_size(ctypes.byref(cfg))), "x")
-    _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
-    _check_size(phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "phi2_toep")
-    if cfg.is_masked and mask is None:
-        raise ValueError("cfg.is_masked is set, so a mask is required")
-    px = _ptr(x, "x", "complex64")
-    ps = _ptr(SEs, "SEs", "complex64")
-    pk = _ptr(phi2_toep, "phi2_toep", "complex64")
-    pm = _ptr(mask, "mask", "int64", allow_none=True)
-    if out is None:
-        out = _empty(_shape(x), "complex64", _device_of(x))
-    else:
-        _check_size(out, _size(x), "out")
-    check(lib.mr_aha_toeplitz(ctypes.byref(cfg), px, ps, pk, pm, _ptr(out, "out", "complex64")),
+    """``A^H A x`` in one call from a ready kernel (the reference's
+    ``aha_toeplitz``): a plan is made, applied once and released."""
+    _validate(cfg, x=x, SEs=SEs, phi2_toep=phi2_toep, mask=mask, out=out)
+    ptrs = (_ptr(x, "x", "complex64"), _ptr(SEs, "SEs", "complex64"),
+            _ptr(phi2_toep, "phi2_toep", "complex64"),
+            _ptr(mask, "mask", "int64", allow_none=True))
+    out = _out_like(x, out)
+    check(lib.mr_aha_toeplitz(ctypes.byref(cfg), *ptrs, _ptr(out, "out", "complex64")),
           "mr_aha_toeplitz")
     return out
 
@@ -338,17 +364,13 @@ class AhAPlan:
     def execute(self, x, SEs, phi2_toep, mask=None, out=None):
         if not self._h:
             raise RuntimeError("this AhAPlan has already been closed")
-        cfg = self._cfg
-        _check_size(x, int(lib.mr_x_size(ctypes.byref(cfg))), "x")
-        _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
-        _check_size(phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "phi2_toep")
-        if out is None:
-            out = _empty(tuple(x.shape), "complex64", _device_of(x))
-        check(lib.mr_aha_plan_execute(self._h, _ptr(x, "x", "complex64"),
-                                      _ptr(SEs, "SEs", "complex64"),
-                                      _ptr(phi2_toep, "phi2_toep", "complex64"),
-                                      _ptr(mask, "mask", "int64", allow_none=True),
-                                      _ptr(out, "out", "complex64")), "mr_aha_plan_execute")
+        _validate(self._cfg, x=x, SEs=SEs, phi2_toep=phi2_toep, mask=mask, out=out)
+        ptrs = (_ptr(x, "x", "complex64"), _ptr(SEs, "SEs", "complex64"),
+                _ptr(phi2_toep, "phi2_toep", "complex64"),
+                _ptr(mask, "mask", "int64", allow_none=True))
+        out = _out_like(x, out)
+        check(lib.mr_aha_plan_execute(self._h, *ptrs, _ptr(out, "out", "complex64")),
+              "mr_aha_plan_execute")
         return out
 
     __call__ = execute
@@ -389,13 +411,42 @@ def _devices_arg(devices):
 _NUFFT_OPTS = ("upsampfac", "gpu_method")
 
 
+def _op_options(kind: int, cfg: MRConfig, devices, toep_dist, share_primary: bool,
+                nufft_opts) -> tuple:
+    """``mr_op_options`` of a create call, and the device list array it
+    points to (kept alive by the caller until ``mr_op_create`` returns).
+    NUFFT settings belong to ``method='nufft'`` only, which has no kernel and
+    so no mask."""
+    extra = dict(nufft_opts or {})
+    if kind == OpMethod.NUFFT:
+        if cfg.is_masked:
+            raise ValueError("method='nufft' has no kernel to mask; build the configuration "
+                             "with is_masked=False")
+        unknown = sorted(set(extra) - set(_NUFFT_OPTS))
+        if unknown:
+            raise ValueError(f"unknown nufft_opts {unknown}; accepted: {list(_NUFFT_OPTS)}")
+    elif extra:
+        raise ValueError("nufft_opts is only used with method='nufft'")
+    dev_array, n_dev = _devices_arg(devices)
+    opt = MROpOptions()
+    check(lib.mr_op_options_defaults(ctypes.byref(opt)), "mr_op_options_defaults")
+    opt.method = kind
+    opt.devices = ctypes.cast(dev_array, ctypes.POINTER(ctypes.c_int)) if dev_array else None
+    opt.n_devices = n_dev
+    opt.toep_dist = ToepDist.parse(toep_dist)
+    opt.flags = OP_SHARE_PRIMARY if share_primary else 0
+    opt.nufft_upsampfac = float(extra.get("upsampfac", 0.0))
+    opt.nufft_gpu_method = int(extra.get("gpu_method", 0))
+    return opt, dev_array
+
+
 class AhAOp:
-    """The ``A^H A`` operator (reference ``api.py:745-1235``).
+    """The ``A^H A`` operator (the reference's ``AhAOp``).
 
     ``op = create_op(cfg, SEs, phi2, traj)`` builds the Toeplitz kernel on the
-    GPU and a plan; ``op(x)`` applies it on ``cfg.stream``. ``method='nufft'``
-    is rejected by the library (MR_ERR_UNSUPPORTED). One GPU: ``devices``
-    other than the primary are accepted and served by the primary alone.
+    GPU and a plan; ``op(x)`` applies it on ``cfg.stream``. One GPU:
+    ``devices`` other than the primary are accepted and served by the
+    primary alone.
     """
 
     def __init__(self, *args, **kwargs):
@@ -409,65 +460,39 @@ class AhAOp:
                   kernel_format: str = "complex64", keep_complex64: bool = True) -> "AhAOp":
         """Create the operator (``mr_op_create``).
 
-        ``kernel_format`` (``'complex64'``, ``'bf16'`` or ``'int16'``) selects
-        the storage of the kernel read by every apply (no reference
-        counterpart; see ``mr_b200_op_set_kernel_format``).
+        The operator is built from the Gram blocks ``phi2`` at ``traj``, or,
+        for ``method='toeplitz'`` with ``phi2`` and ``traj`` both None, from a
+        ready kernel ``_phi2_toep``. ``kernel_format`` (``'complex64'``,
+        ``'bf16'`` or ``'int16'``) selects the storage of the kernel read by
+        every apply (no reference counterpart; ``mr_b200_op_set_kernel_format``).
         """
+        kind = OpMethod.parse(method)
+        opt, dev_array = _op_options(kind, cfg, devices, toep_dist, share_primary, nufft_opts)
+        if _phi2_toep is not None and kind == OpMethod.NUFFT:
+            raise ValueError("_phi2_toep is only used with method='toeplitz'")
+        from_kernel = _phi2_toep is not None and phi2 is None and traj is None
+        if not from_kernel and (phi2 is None or traj is None):
+            raise ValueError("phi2 and traj are required (the operator is built from the "
+                             "Gram blocks)")
+        n_traj, n_kx = _validate(cfg, SEs=SEs, phi2=phi2, traj=traj, mask=mask,
+                                 _phi2_toep=_phi2_toep)
+        inputs = MROpInputs(
+            d_SEs=_ptr(SEs, "SEs", "complex64"),
+            d_phi2=_ptr(phi2, "phi2", "complex64", allow_none=from_kernel),
+            d_traj=_ptr(traj, "traj", "float32", allow_none=from_kernel),
+            Ntrajs=n_traj, Nkx=n_kx,
+            d_mask=_ptr(mask, "mask", "int64", allow_none=True),
+            d_phi2_toep=_ptr(_phi2_toep, "_phi2_toep", "complex64", allow_none=True))
         self = cls.__new__(cls)
         self._handle = ctypes.c_void_p()
-        self._keep = ()
-        self._method = OpMethod._TO_STR[OpMethod.parse(method)]
-        is_nufft = self._method == "nufft"
-        if is_nufft and cfg.is_masked:
-            raise ValueError("method='nufft' has no kernel to mask; build the configuration "
-                             "with is_masked=False")
-        nufft_opts = dict(nufft_opts or {})
-        if not is_nufft and nufft_opts:
-            raise ValueError("nufft_opts is only used with method='nufft'")
-        unknown = set(nufft_opts) - set(_NUFFT_OPTS)
-        if unknown:
-            raise ValueError(f"unknown nufft_opts {sorted(unknown)}; accepted: {list(_NUFFT_OPTS)}")
-        _check_size(SEs, int(lib.mr_se_size(ctypes.byref(cfg))), "SEs")
-        if _phi2_toep is not None and phi2 is None and traj is None and not is_nufft:
-            Ntrajs, Nkx = 0, 0
-            if cfg.is_masked:
-                if mask is None:
-                    raise ValueError("cfg.is_masked is set, so a mask is required")
-                if cfg.num_masked == 0:
-                    cfg.num_masked = _size(mask)
-        else:
-            if phi2 is None or traj is None:
-                raise ValueError("phi2 and traj are required (the operator is built from the "
-                                 "Gram blocks)")
-            Ntrajs, Nkx = _check_gram(cfg, phi2, traj, mask)
-        if _phi2_toep is not None:
-            if is_nufft:
-                raise ValueError("_phi2_toep is only used with method='toeplitz'")
-            _check_size(_phi2_toep, int(lib.mr_phi2_toep_size(ctypes.byref(cfg))), "_phi2_toep")
-        devs, ndev = _devices_arg(devices)
+        self._method = OpMethod._TO_STR[kind]
         self._cfg = MRConfig.from_buffer_copy(cfg)
-        opt = MROpOptions()
-        check(lib.mr_op_options_defaults(ctypes.byref(opt)), "mr_op_options_defaults")
-        opt.method = OpMethod.parse(method)
-        opt.devices = ctypes.cast(devs, ctypes.POINTER(ctypes.c_int)) if devs else None
-        opt.n_devices = ndev
-        opt.toep_dist = ToepDist.parse(toep_dist)
-        opt.flags = OP_SHARE_PRIMARY if share_primary else 0
-        opt.nufft_upsampfac = float(nufft_opts.get("upsampfac", 0.0))
-        opt.nufft_gpu_method = int(nufft_opts.get("gpu_method", 0))
-        inp = MROpInputs(
-            _ptr(SEs, "SEs", "complex64"),
-            _ptr(phi2, "phi2", "complex64", allow_none=_phi2_toep is not None),
-            _ptr(traj, "traj", "float32", allow_none=_phi2_toep is not None),
-            int(Ntrajs), int(Nkx),
-            _ptr(mask, "mask", "int64", allow_none=True),
-            _ptr(_phi2_toep, "_phi2_toep", "complex64", allow_none=True),
-        )
-        if share_primary:
-            self._keep = (SEs, mask, _phi2_toep)
         self._device = _device_of(SEs)
-        check(lib.mr_op_create(ctypes.byref(cfg), ctypes.byref(inp), ctypes.byref(opt),
+        # arrays the library may keep using in place (MR_OP_SHARE_PRIMARY)
+        self._keep = (SEs, mask, _phi2_toep) if share_primary else ()
+        check(lib.mr_op_create(ctypes.byref(cfg), ctypes.byref(inputs), ctypes.byref(opt),
                                ctypes.byref(self._handle)), "mr_op_create")
+        del dev_array
         if kernel_format != "complex64":
             self.set_kernel_format(kernel_format, keep_complex64=keep_complex64)
         return self
@@ -487,12 +512,9 @@ class AhAOp:
     def apply(self, x, out=None):
         """``A^H A x`` (``mr_op_execute``), ordered on ``cfg.stream``."""
         self._check_open()
-        _check_size(x, int(lib.mr_x_size(ctypes.byref(self._cfg))), "x")
+        _validate(self._cfg, need_mask=False, x=x, out=out)
         px = _ptr(x, "x", "complex64")
-        if out is not None:
-            _check_size(out, _size(x), "out")
-        else:
-            out = _empty(_shape(x), "complex64", _device_of(x))
+        out = _out_like(x, out)
         check(lib.mr_op_execute(self._handle, px, _ptr(out, "out", "complex64")),
               "mr_op_execute")
         return out

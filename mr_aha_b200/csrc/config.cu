@@ -5,13 +5,44 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <string>
 
 #include "mr_internal.h"
+#include "mr_aha/mr_aha_b200.h"
 
 namespace {
 constexpr int kErrLen = 512;
 thread_local char g_err[kErrLen] = {0};
+thread_local std::string g_trace;
 }  // namespace
+
+thread_local int mr_trace_on = 0;
+
+void mr_trace_note(const char *fmt, ...) {
+    char line[160];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(line, sizeof(line), fmt, ap);
+    va_end(ap);
+    g_trace += line;
+    g_trace += '\n';
+}
+
+extern "C" int mr_b200_trace_launches(int enable) {
+    mr_clear_error();
+    if (enable) g_trace.clear();
+    mr_trace_on = enable ? 1 : 0;
+    return MR_SUCCESS;
+}
+
+extern "C" int64_t mr_b200_trace_read(char *buf, size_t cap) {
+    if (buf && cap > 0) {
+        const size_t n = g_trace.size() < cap - 1 ? g_trace.size() : cap - 1;
+        std::memcpy(buf, g_trace.data(), n);
+        buf[n] = '\0';
+    }
+    return (int64_t)g_trace.size();
+}
 
 void mr_set_error(const char *fmt, ...) {
     va_list ap;

@@ -41,12 +41,31 @@ void mr_clear_error();
         }                                                                       \
     } while (0)
 
-#define MR_LAUNCH_CHECK(name)                                                   \
+// Launch trace of the calling thread (mr_b200_trace_launches): while it is
+// on, every launch appends one line naming the kernel (the specialised
+// launchers name their template arguments).
+extern thread_local int mr_trace_on;
+void mr_trace_note(const char *fmt, ...);
+
+#define MR_LAUNCH_ERR(name)                                                     \
     do {                                                                        \
         cudaError_t mr_e_ = cudaGetLastError();                                 \
         if (mr_e_ != cudaSuccess)                                               \
             MR_FAIL(MR_ERR_CUDA, "kernel %s failed to launch: %s", name,        \
                     cudaGetErrorString(mr_e_));                                 \
+    } while (0)
+
+#define MR_LAUNCH_CHECK(name)                                                   \
+    do {                                                                        \
+        if (mr_trace_on) mr_trace_note("%s", name);                             \
+        MR_LAUNCH_ERR(name);                                                    \
+    } while (0)
+
+// As MR_LAUNCH_CHECK, tracing a printf-style description of the launch.
+#define MR_LAUNCH_CHECK_T(name, ...)                                            \
+    do {                                                                        \
+        if (mr_trace_on) mr_trace_note(__VA_ARGS__);                            \
+        MR_LAUNCH_ERR(name);                                                    \
     } while (0)
 
 // Geometry of one operator, passed by value to the kernels.

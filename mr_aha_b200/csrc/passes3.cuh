@@ -610,7 +610,7 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
             const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
             k_hf_pipe<N, XT, kNT, 2, PG><<<(unsigned)nb, kNT, (size_t)4 * N * XT * sizeof(float2),
                                            s>>>(a);
-            MR_LAUNCH_CHECK("k_hf_pipe");
+            MR_LAUNCH_CHECK_T("k_hf_pipe", "k_hf_pipe<N=%d,XT=%d>", N, XT);
             return MR_SUCCESS;
         }
     }
@@ -623,7 +623,7 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
             const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
             k_hi_pipe<N, XT, kNT, 3, PG><<<(unsigned)nb, kNT, (size_t)6 * N * XT * sizeof(float2),
                                            s>>>(a);
-            MR_LAUNCH_CHECK("k_hi_pipe");
+            MR_LAUNCH_CHECK_T("k_hi_pipe", "k_hi_pipe<N=%d,XT=%d>", N, XT);
             return MR_SUCCESS;
         }
     }
@@ -634,7 +634,8 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
         set_attr(k_strided_hi<N, XT, kNT, MINB>, attr);
         k_strided_hi<N, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
     }
-    MR_LAUNCH_CHECK("k_strided_h");
+    MR_LAUNCH_CHECK_T("k_strided_h", "%s<N=%d,XT=%d>", DIR < 0 ? "k_strided_hf" : "k_strided_hi",
+                      N, XT);
     return MR_SUCCESS;
 }
 
@@ -795,7 +796,7 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
             if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
             k_xs_pipe<M, XT, 256, PB><<<(unsigned)nb, 256, (size_t)4 * M * XT * sizeof(float2),
                                         s>>>(a);
-            MR_LAUNCH_CHECK("k_xs_pipe");
+            MR_LAUNCH_CHECK_T("k_xs_pipe", "k_xs_pipe<M=%d,XT=%d>", M, XT);
             return MR_SUCCESS;
         }
     }
@@ -811,7 +812,7 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
             if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
             k_coilsum_pipe<M, XT, 256, PB><<<(unsigned)nb, 256,
                                              (size_t)6 * M * XT * sizeof(float2), s>>>(a);
-            MR_LAUNCH_CHECK("k_coilsum_pipe");
+            MR_LAUNCH_CHECK_T("k_coilsum_pipe", "k_coilsum_pipe<M=%d,XT=%d>", M, XT);
             return MR_SUCCESS;
         }
     }
@@ -823,7 +824,8 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
     if (nblk <= 0) return MR_SUCCESS;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
     k_strided3<DIR, LM, SM, M, XT, kNT, MINB><<<(unsigned)nblk, kNT, smem, s>>>(a);
-    MR_LAUNCH_CHECK("k_strided3");
+    MR_LAUNCH_CHECK_T("k_strided3", "k_strided3<%s,M=%d,XT=%d,LM=%d,SM=%d>",
+                      DIR < 0 ? "fwd" : "inv", M, XT, LM, SM);
     return MR_SUCCESS;
 }
 
@@ -836,7 +838,7 @@ int launch_x3(const mr_x_args &a, cudaStream_t s) {
     const int64_t nblk = (int64_t)a.nloc * a.nchunk;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
     k_xbd3<M, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
-    MR_LAUNCH_CHECK("k_xbd3");
+    MR_LAUNCH_CHECK_T("k_xbd3", "k_xbd3<M=%d,L=%d,NC=%d,KF=%d>", M, L, NC, KF);
     return MR_SUCCESS;
 }
 
@@ -851,14 +853,16 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
             static unsigned long long attr_b = 0;
             set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
             k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);
-            MR_LAUNCH_CHECK("k_xbdh");
+            MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked>", N, L, NC, kNT);
             return MR_SUCCESS;
         }
     }
     static unsigned long long attr = 0;
     set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
     k_xbdh<N, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
-    MR_LAUNCH_CHECK("k_xbdh");
+    MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,%s,%d%s>", N, L, NC,
+                      KF == MR_KF_F32 ? "F32" : (KF == MR_KF_BF16 ? "BF16" : "I16"), kNT,
+                      a.K.inv ? ",masked" : "");
     return MR_SUCCESS;
 }
 

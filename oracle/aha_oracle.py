@@ -284,6 +284,49 @@ def aha_toeplitz(traj_type: str, n_dim, phi2_dim, L: int, x: np.ndarray,
     return out
 
 
+def aha_toeplitz_lean(traj_type: str, n_dim, phi2_dim, L: int, x: np.ndarray,
+                      SEs: np.ndarray, phi2_toep: np.ndarray, upper: bool = False) -> np.ndarray:
+    """FP64 Toeplitz ``A^H A x`` for grids too large for :func:`aha_toeplitz`'s
+    full ``L x L`` blocks (unmasked kernels only).
+
+    The same arithmetic as :func:`aha_toeplitz` (``mr_aha.cu:694-790``), one
+    coil at a time: the spectrum is moved to centred order
+    (``fftshift``, the inverse of the kernel's ``nat2cent`` read,
+    ``mr_kernels.cu:178-219``) and multiplied by walking the packed triangle
+    in place (``mr_kernels_bd.cu:56-139``: ``y_c += A_rc v_r`` and, off the
+    diagonal, ``y_r += conj(A_rc) v_c``), so no expanded block array exists;
+    the packed kernel is read as given (complex64 values are exact in
+    complex128)."""
+    img = spatial_axes(traj_type, n_dim)
+    m_pad = spatial_axes(traj_type, phi2_dim)
+    ntri = num_tri(L)
+    x = np.asarray(x, dtype=np.complex128).reshape((L,) + img)
+    S = np.asarray(SEs).reshape((-1,) + img)
+    K = np.asarray(phi2_toep).reshape((ntri,) + m_pad)
+    rows, cols = tri_pairs(L, upper)
+    ix = np.ix_(*pad_index_maps(img, m_pad))
+    axes = tuple(range(1, 1 + len(img)))
+    out = np.zeros((L,) + img, dtype=np.complex128)
+    for c in range(S.shape[0]):
+        Sc = S[c].astype(np.complex128)
+        pad = np.zeros((L,) + m_pad, dtype=np.complex128)
+        pad[(slice(None),) + ix] = Sc[None] * x
+        v = np.fft.fftshift(np.fft.fftn(pad, axes=axes), axes=axes)
+        del pad
+        y = np.zeros_like(v)
+        for t in range(ntri):
+            r, cc = int(rows[t]), int(cols[t])
+            a = K[t]
+            y[cc] += a * v[r]
+            if r != cc:
+                y[r] += np.conj(a) * v[cc]
+        del v
+        back = np.fft.ifftn(np.fft.ifftshift(y, axes=axes), axes=axes) * np.prod(m_pad)
+        del y
+        out += np.conj(Sc)[None] * back[(slice(None),) + ix]
+    return out
+
+
 # --------------------------------------------------------------------------
 # NUFFT route (python/mr_aha/nufft.py:473-552), exact NUDFTs
 # --------------------------------------------------------------------------

@@ -4,10 +4,11 @@ Callers that cannot allocate device memory (their GPU memory is owned by
 their own pool, or their processing loop must not synchronise or risk an
 out-of-memory failure) use this entry point; it takes its work space from
 the library's fixed static scratch array. Through the C ABI, two calls in a
-row must each match mr_aha_toeplitz, the allocating entry point, within the
-apply tolerance of the parity tests (1e-5 relative L2); the second call also
-checks that the contents left in the shared array by the first do not leak
-into the result. Collected last (file name) so that a run stopping at the
+row must each match mr_aha_toeplitz, the allocating entry point, and the
+FP64 oracle's apply of the same inputs (oracle.aha_oracle.aha_toeplitz),
+within the apply tolerance of the parity tests (1e-5 relative L2); the
+second call also checks that the contents left in the shared array by the
+first do not leak into the result. Collected last (file name) so that a run stopping at the
 first failure has run every other test first; it also passes on its own.
 """
 
@@ -17,6 +18,7 @@ import numpy as np
 import pytest
 
 from mr_aha_b200 import synth
+from oracle import aha_oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -57,6 +59,9 @@ def test_noalloc_matches_allocating_apply(case, masked):
     x = torch.from_numpy(p["x"]).to(dev)
     S = torch.from_numpy(p["SEs"]).to(dev)
     ref = mr.aha_toeplitz(cfg, x, S, K, mask=mask).cpu().numpy()
+    ref64 = O.aha_toeplitz(p["traj_type"], p["n_dim"], p["phi2_dim"], p["L"], p["x"],
+                           p["SEs"], K.cpu().numpy(),
+                           mask=None if mask is None else mask.cpu().numpy())
     for call in range(2):
         out = torch.full_like(x, complex(float("nan"), 0.0))
         rc = lib.mr_b200_aha_toeplitz_noalloc(
@@ -65,7 +70,9 @@ def test_noalloc_matches_allocating_apply(case, masked):
             _ptr(out, "out", "complex64"))
         assert rc == 0, lib.mr_last_error()
         torch.cuda.synchronize()
-        assert _rel(out.cpu().numpy(), ref) <= TOL, f"call {call}"
+        y = out.cpu().numpy()
+        assert _rel(y, ref) <= TOL, f"call {call}: vs the allocating apply"
+        assert O.rel_l2(y, ref64) <= TOL, f"call {call}: vs the FP64 oracle"
 
 
 def test_noalloc_rejects_oversized_problem():
