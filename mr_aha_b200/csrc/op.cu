@@ -8,7 +8,8 @@
 // MR_OP_SHARE_PRIMARY, borrows) the maps, the mask and the kernel, and an
 // apply plan. Its kernel can be converted to 16-bit storage with a per-
 // location scale (mr_b200_op_set_kernel_format), in which case the applies
-// read the 16-bit copy.
+// read the 16-bit copy. An MR_OP_NUFFT operator holds no kernel and no plan:
+// its applies run the NUFFT engine of nufft.cu.
 #include <algorithm>
 #include <chrono>
 #include <new>
@@ -16,6 +17,7 @@
 
 #include "engine.h"
 #include "mr_aha/mr_aha_b200.h"
+#include "nufft.h"
 
 struct mr_op_s {
     mr_config cfg;
@@ -34,6 +36,7 @@ struct mr_op_s {
     int kf;
     void *K16;
     float *K16_scale;
+    mr_nufft_op *nu;        // MR_OP_NUFFT engine, NULL for the Toeplitz method
     mr_op_info_t info;
 };
 
@@ -46,6 +49,7 @@ static void op_release(mr_op op, int skip_device) {
         if (op->K16) cudaFree(op->K16);
         if (op->K16_scale) cudaFree(op->K16_scale);
         if (op->K_blk) cudaFree(op->K_blk);
+        mr_nufft_op_destroy(op->nu);
         cudaGetLastError();
     }
     delete op;
@@ -138,9 +142,9 @@ static int op_check(const mr_config *cfg, const mr_op_inputs *in, const mr_op_op
                    "(or use the Toeplitz method)");
         MR_REQUIRE(in->d_phi2_toep == nullptr,
                    "mr_op_create: d_phi2_toep is only used by the Toeplitz method");
-        MR_FAIL(MR_ERR_UNSUPPORTED,
-                "mr_op_create: the NUFFT method is not built in this library; use "
-                "MR_OP_TOEPLITZ");
+        MR_REQUIRE(o->nufft_upsampfac == 0.0 || o->nufft_upsampfac > 1.0,
+                   "mr_op_create: nufft_upsampfac = %g must be 0 (default 2.0) or above 1",
+                   o->nufft_upsampfac);
     }
     if (cfg->is_masked)
         MR_REQUIRE(in->d_mask != nullptr, "mr_op_create: d_mask is required when is_masked is set");
@@ -185,6 +189,34 @@ static int op_create_impl(const mr_config *cfg, const mr_op_inputs *in, const mr
         op->mask = (const int64_t *)op->mask_own;
     }
     double toep_ms = 0.0;
+    if (o->method == MR_OP_NUFFT) {
+        mr_config c = *cfg;
+        c.gpu_device_id = -1;
+        rc = mr_nufft_op_create(&c, reinterpret_cast<const float2 *>(in->d_phi2), in->d_traj,
+                                in->Ntrajs, in->Nkx, o->nufft_upsampfac, s, &op->nu);
+        if (rc != MR_SUCCESS) {
+            char msg[512];
+            snprintf(msg, sizeof(msg), "%s", mr_last_error());
+            op_release(op, 0);
+            mr_set_error("%s", msg);
+            return rc;
+        }
+        op->kf = MR_KF_F32;
+        mr_op_info_t &inf = op->info;
+        inf.method = MR_OP_NUFFT;
+        inf.n_devices = 1;
+        inf.devices[0] = op->dev;
+        inf.coil_begin[0] = 0;
+        inf.coil_count[0] = cfg->n_coils;
+        inf.group[0] = 1;
+        inf.toep_source = MR_OP_TOEP_NONE;
+        inf.toep_devices = 0;
+        inf.create_ms = std::chrono::duration<double, std::milli>(
+                            std::chrono::steady_clock::now() - t_start)
+                            .count();
+        *out = op;
+        return MR_SUCCESS;
+    }
     if (in->d_phi2_toep) {
         if (share) {
             op->K = reinterpret_cast<const float2 *>(in->d_phi2_toep);
@@ -303,6 +335,7 @@ static mr_kernel_ref op_kernel_ref(mr_op op) {
 }
 
 int mr_op_execute_on(mr_op op, const float2 *x, float2 *out, cudaStream_t s) {
+    if (op->nu) return mr_nufft_op_apply(op->nu, x, op->S, out, s);
     return mr_plan_execute_k(op->plan, x, op->S, op_kernel_ref(op), op->mask, out, s);
 }
 
@@ -419,6 +452,8 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
     MR_REQUIRE(format == MR_B200_KF_COMPLEX64 || format == MR_B200_KF_BF16 ||
                    format == MR_B200_KF_INT16,
                "mr_b200_op_set_kernel_format: unknown format %d", format);
+    if (op->nu)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "mr_b200_op_set_kernel_format: a NUFFT operator has no kernel");
     int prev = 0;
     MR_CUDA_TRY(cudaGetDevice(&prev));
     if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
@@ -491,6 +526,8 @@ extern "C" int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d
     mr_clear_error();
     MR_REQUIRE(op && d_x && d_AhAx && ms && n_passes, "mr_b200_op_profile: NULL argument");
     MR_REQUIRE(max_passes >= 1, "mr_b200_op_profile: max_passes must be >= 1");
+    if (op->nu)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "mr_b200_op_profile: per-pass timing is for Toeplitz operators");
     int prev = 0;
     MR_CUDA_TRY(cudaGetDevice(&prev));
     if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
@@ -530,6 +567,8 @@ extern "C" int mr_b200_op_autotune(mr_op op, int reps, float *ms) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr, "mr_b200_op_autotune: op is NULL");
     MR_REQUIRE(reps >= 1 && reps <= 100, "mr_b200_op_autotune: reps = %d outside [1, 100]", reps);
+    if (op->nu)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "mr_b200_op_autotune: a NUFFT operator has no pass choices");
     int prev = 0;
     MR_CUDA_TRY(cudaGetDevice(&prev));
     if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
@@ -562,6 +601,10 @@ extern "C" int mr_b200_op_autotune(mr_op op, int reps, float *ms) {
 extern "C" int mr_b200_op_blocked_copy(mr_op op, int enable, int *built) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr, "mr_b200_op_blocked_copy: op is NULL");
+    if (op->nu) {
+        if (built) *built = 0;
+        return MR_SUCCESS;
+    }
     int prev = 0;
     MR_CUDA_TRY(cudaGetDevice(&prev));
     if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
@@ -589,6 +632,7 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     if (op->K_blk) b += nloc * ntri * sizeof(float2);
     if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
     if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
+    b += mr_nufft_op_bytes(op->nu);
     *bytes = b;
     return MR_SUCCESS;
 }
@@ -596,6 +640,8 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
 extern "C" int mr_b200_op_launches(mr_op op, int *n) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");
-    *n = mr_plan_launch_count(op->plan);
+    // NUFFT operator: per coil, 4 (+2 for a stack) kernels around the NUFFTs,
+    // each NUFFT 5 (2-D) or 6 (3-D) kernels per plane chunk
+    *n = op->plan ? mr_plan_launch_count(op->plan) : 0;
     return MR_SUCCESS;
 }

@@ -24,6 +24,7 @@
 // the result is rounded once to complex64. Cost: Ntrajs*Nkx*prod(M) for the
 // per-readout PSFs plus ntri*Nkz*Ntrajs*prod(M) for the contraction.
 #include "engine.h"
+#include "nufft.h"
 
 #include <algorithm>
 #include <cmath>
@@ -232,6 +233,81 @@ struct dev_buf {
 
 }  // namespace
 
+static int from_psf_impl(const mr_config *cfg, const float2 *psf, int64_t t0, int64_t n,
+                         const int64_t *mask, float2 *out_all);
+
+// Kernel build by spreading, for geometries where the closed form's
+// Ntrajs * Nkx * prod(M) cost is prohibitive (3-D kooshball grids): per
+// packed component t (and kz plane of a stack), the type-1 non-uniform FFT
+// (sign -1, centred modes phi2_dim) of the strengths c_{t,m} (component t of
+// sample m's readout Gram block, broadcast along the readout) with FP64
+// accumulation in the spreading step (nufft.cu), then the centred inverse
+// FFT / prod(M) (from_psf_impl) -- the reference's pipeline
+// (src/cuda/mr_calc_toep.cu:537-633) with this library's own NUFFT. Writes
+// components [t0, t0 + nt) to out (component t0 first).
+static int toep_spread_build(const mr_config *cfg, const double2 *T, const float *traj,
+                             int64_t Ntrajs, int64_t Nkx, float2 *out, int64_t t0, int64_t nt,
+                             cudaStream_t s) {
+    const bool three = cfg->traj_type == MR_TRAJ_3D;
+    const int Mx = cfg->phi2_dim[0], My = cfg->phi2_dim[1], Mz = cfg->phi2_dim[2];
+    const int nkz = cfg->traj_type == MR_TRAJ_STACK ? Mz : 1;
+    const int modes[3] = {Mx, My, Mz};
+    const int dims = three ? 3 : 2;
+    const double eps = std::min(cfg->eps > 0 ? cfg->eps : 1e-6, 1e-7);
+    const int64_t vpad = mr_pad_size(cfg);
+    size_t budget = 0;
+    int rc = mr_memory_budget(cfg, &budget);
+    if (rc != MR_SUCCESS) return rc;
+    // planes per call: whole components (nkz planes each) within the budget
+    const size_t per_comp = mr_nufft_plan_bytes(dims, modes, eps, 2.0, nkz, 1);
+    int64_t tc = (int64_t)std::max<size_t>(1, (budget / 2) / std::max<size_t>(per_comp, 1));
+    tc = std::min<int64_t>(std::min<int64_t>(tc, nt), 64);
+    const int env_c = mr_env_int("MR_AHA_TOEP_MAX_CHUNK", 0);
+    if (env_c > 0) tc = std::min<int64_t>(tc, env_c);
+    mr_nufft *plan = nullptr;
+    rc = mr_nufft_create(dims, modes, traj, Ntrajs * Nkx, eps, 2.0, (int)(tc * nkz), 1, &plan);
+    if (rc != MR_SUCCESS) return rc;
+    dev_buf psf;
+    rc = psf.alloc((size_t)tc * vpad * sizeof(float2), "the spread PSFs");
+    mr_config c = *cfg;
+    c.is_masked = 0;
+    c.num_masked = 0;
+    for (int64_t a = 0; a < nt && rc == MR_SUCCESS; a += tc) {
+        const int64_t n = std::min(tc, nt - a);
+        // planes (t, kz) of components [t0 + a, t0 + a + n): strengths
+        // T[(t nkz + kz) Ntrajs + s], sample m of readout s = m % Ntrajs
+        rc = mr_nufft_type1(plan, -1, T + (t0 + a) * nkz * Ntrajs, Ntrajs, Ntrajs,
+                            (int)(n * nkz), (float2 *)psf.p, s);
+        if (rc == MR_SUCCESS) rc = from_psf_impl(&c, (const float2 *)psf.p, a, n, nullptr, out);
+    }
+    cudaStreamSynchronize(s);
+    mr_nufft_destroy(plan);
+    return rc;
+}
+
+// Which build a configuration takes: MR_AHA_B200_TOEP_METHOD = 1 forces the
+// spreading build, 2 the closed form; otherwise the cheaper by a cost model
+// calibrated on B200 (3-D 64^3 image, 128^3 grid, L = 4, 2000 x 128
+// samples: closed form 0.59 s, about 8 TFLOP/s of FP64 GEMM; spreading
+// 0.04 s, about 9e10 double atomic adds per second, taken as 5e10 here).
+static bool use_spread_build(const mr_config *cfg, int64_t Ntrajs, int64_t Nkx) {
+    const int m = mr_env_int("MR_AHA_B200_TOEP_METHOD", 0);
+    if (m == 1) return true;
+    if (m == 2) return false;
+    const bool three = cfg->traj_type == MR_TRAJ_3D;
+    const double Mx = cfg->phi2_dim[0], My = cfg->phi2_dim[1], Mz = cfg->phi2_dim[2];
+    const double nkz = cfg->traj_type == MR_TRAJ_STACK ? Mz : 1;
+    const double ntri = (double)mr_num_tri(cfg->L);
+    const double grid = Mx * My * (three ? Mz : 1);
+    const double smp = (double)Ntrajs * Nkx;
+    const double t_exact = 8.0 * (smp * grid + ntri * nkz * Ntrajs * grid) / 8e12;
+    const double w = 9, wd = three ? w * w * w : w * w;
+    const double fine = grid * (three ? 8.0 : 4.0);
+    const double t_spread =
+        ntri * nkz * (2.0 * smp * wd / 5e10 + 10.0 * fine * std::log2(fine) / 5e12);
+    return t_spread < t_exact;
+}
+
 // Build the unmasked kernel rows [row0, row0 + nrows) of the output matrix
 // (rows = components for 2D / 3D, (component, kz) for a stack) into
 // `out` (row stride = columns), or all rows when nrows < 0.
@@ -258,6 +334,8 @@ static int toep_build(const mr_config *cfg, const float2 *phi2, const float *tra
     k_pack_gram<<<grid_for(nbatch * L * L), 256, 0, s>>>(T, phi2, nbatch, L,
                                                         cfg->triangulation == MR_TRI_UPPER);
     MR_LAUNCH_CHECK("k_pack_gram");
+    if (use_spread_build(cfg, Ntrajs, Nkx))
+        return toep_spread_build(cfg, T, traj, Ntrajs, Nkx, out, t0, nt, s);
 
     // Memory plan: Ks for all readouts over a chunk of PSF rows, plus the
     // Dirichlet tables of a chunk of readouts.
