@@ -615,10 +615,60 @@ def run_serve(args):
     return 0
 
 
+def run_toep(args):
+    """Kernel build (mr_calc_toep) timed both ways: the closed form (FP64
+    GEMMs) and the spreading build (ES-kernel type-1 NUFFT with FP64
+    accumulation), on the headline stack and on a 3-D kooshball grid
+    (128^3 image, 256^3 grid, L = 4, 10000 spokes of 256 samples), with the
+    two results compared (relative L2)."""
+    import os
+
+    import torch
+
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    cases = {
+        "stack320": synth.workload("stack320", with_x=False),
+        "kooshball128": synth.spec_inputs(dict(traj_type="3D", n_dim=(128, 128, 128), L=4,
+                                               n_coils=1, n_traj=10000, n_kx=256,
+                                               n_frames=200, frame_rule="div", seed=41),
+                                          with_x=False),
+    }
+    out = {}
+    for name, w in cases.items():
+        cfg = mr.make_config(w["traj_type"], w["n_dim"], w["L"], n_coils=w["n_coils"],
+                             mem_fraction=0.6)
+        phi2 = torch.from_numpy(w["phi2"]).to(dev)
+        traj = torch.from_numpy(w["traj"]).to(dev)
+        res, Ks = {}, {}
+        for method, code in (("spread", "1"), ("closed_form", "2")):
+            os.environ["MR_AHA_B200_TOEP_METHOD"] = code
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Ks[method] = mr.calc_toep(cfg, phi2, traj)
+            torch.cuda.synchronize()
+            res[method + "_s"] = time.perf_counter() - t0
+        os.environ.pop("MR_AHA_B200_TOEP_METHOD")
+        res["rel_l2_spread_vs_closed_form"] = _rel(Ks["spread"], Ks["closed_form"])
+        res["kernel_gb"] = Ks["spread"].numel() * 8 / 1e9
+        del Ks
+        torch.cuda.empty_cache()
+        out[name] = res
+    line = {"metric": "Toeplitz kernel build time", "value": out["kooshball128"]["spread_s"],
+            "unit": "s", "n_gpus": 1, "higher_is_better": False, "data": "synthetic",
+            "dtype": "FP64 accumulation, complex64 result",
+            "config": {"workload": "toep", "cases": list(cases)}, "builds": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
-        if args.workload in ("cg320", "batch48", "serve"):
+        if args.workload in ("cg320", "batch48", "serve", "toep"):
             print(json.dumps({"impl": "reference", "unavailable":
                               "the reference has no solver, batch or serving loop"}))
             return 0
@@ -629,6 +679,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "toep":
+        return run_toep(args)
     return run_ours(args)
 
 
