@@ -53,6 +53,13 @@ MR_EXPORT int mr_b200_op_blocked_copy(mr_op op, int enable, int *built);
  * buffers); borrowed arrays are not counted. */
 MR_EXPORT int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes);
 
+/* No reference counterpart. Device status of the operator's kernels since the
+ * last call: 0, or MR_B200_DEV_ERR_TMA_TIMEOUT when a kernel gave up a
+ * bounded wait for a TMA copy (its results are then not valid). Reads and
+ * clears the status word; synchronises the operator's stream. */
+#define MR_B200_DEV_ERR_TMA_TIMEOUT 1
+MR_EXPORT int mr_b200_op_device_status(mr_op op, int *status);
+
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 

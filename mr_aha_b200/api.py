@@ -570,6 +570,16 @@ class AhAOp:
         return int(b.value)
 
     @property
+    def device_status(self) -> int:
+        """Status word of the operator's kernels since the last read (0 = no
+        device-side error; ``mr_b200_op_device_status``). Synchronous."""
+        self._check_open()
+        st = ctypes.c_int(0)
+        check(lib.mr_b200_op_device_status(self._handle, ctypes.byref(st)),
+              "mr_b200_op_device_status")
+        return int(st.value)
+
+    @property
     def launches_per_apply(self) -> int:
         self._check_open()
         n = ctypes.c_int(0)

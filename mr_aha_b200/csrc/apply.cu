@@ -39,6 +39,7 @@ struct mr_aha_plan_s {
     int group;       // coils per group
     mr_fft_axis ax[3];
     float2 *d_tw;    // twiddle tables of the three axes
+    int *d_status;   // device status word (MR_DEV_ERR_*), after the tables; NULL if none
     float2 *W0, *W1; // intermediates
     float2 *W2, *W3; // unfused pass 3 only: full-grid spectrum in / out
     int *d_inv;      // masked: natural grid index -> mask row
@@ -199,6 +200,7 @@ static void plan_release(mr_aha_plan p) {
     if (p->W3) cudaFree(p->W3);
     if (p->d_inv) cudaFree(p->d_inv);
     p->d_tw = nullptr;
+    p->d_status = nullptr;
     p->W0 = p->W1 = p->W2 = p->W3 = nullptr;
     p->d_inv = nullptr;
     cudaGetLastError();
@@ -274,7 +276,8 @@ static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
     }
     std::vector<float2> h(tot);
     for (int d = 0; d < 3; ++d) mr_fft_twiddles(g.m[d], h.data() + off[d]);
-    if (cudaMalloc(&p->d_tw, tot * sizeof(float2)) != cudaSuccess) {
+    // the tables, then one 16-byte slot for the device status word
+    if (cudaMalloc(&p->d_tw, (tot + 2) * sizeof(float2)) != cudaSuccess) {
         cudaGetLastError();
         free(p);
         MR_FAIL(MR_ERR_ALLOC, "failed to allocate the FFT tables");
@@ -286,6 +289,12 @@ static int plan_create_impl(const mr_config *cfg, mr_aha_plan *out) {
         MR_FAIL(MR_ERR_CUDA, "failed to upload the FFT tables");
     }
     for (int d = 0; d < 3; ++d) p->ax[d].tw = p->d_tw + off[d];
+    p->d_status = reinterpret_cast<int *>(p->d_tw + tot);
+    if (cudaMemset(p->d_status, 0, 2 * sizeof(float2)) != cudaSuccess) {
+        plan_release(p);
+        free(p);
+        MR_FAIL(MR_ERR_CUDA, "failed to clear the plan's status word");
+    }
 
     // Pass geometry: strided tile widths and the fused pass 3.
     const size_t lim = (size_t)mr_smem_limit();
@@ -373,6 +382,15 @@ extern "C" int mr_aha_plan_destroy(mr_aha_plan plan) {
 int mr_plan_group(mr_aha_plan plan) { return plan->group; }
 cudaStream_t mr_plan_stream(mr_aha_plan plan) { return plan->stream; }
 int mr_plan_launch_count(mr_aha_plan plan) { return plan->launches; }
+
+int mr_plan_device_status(mr_aha_plan p, int *status) {
+    *status = 0;
+    if (!p->d_status) return MR_SUCCESS;
+    MR_CUDA_TRY(cudaStreamSynchronize(p->stream));
+    MR_CUDA_TRY(cudaMemcpy(status, p->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    MR_CUDA_TRY(cudaMemset(p->d_status, 0, sizeof(int)));
+    return MR_SUCCESS;
+}
 
 // ---------------------------------------------------------------------------
 // Execution
@@ -544,6 +562,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.cmy = g.cm[1];
                 a.cmz = g.cm[2];
                 a.K = K;
+                a.status = p->d_status;
                 if (p->nch > 0) {
                     a.nc = p->nch;
                     a.nchunk = (int)mr_cdiv(G, a.nc);

@@ -3,6 +3,7 @@
 // precision / CG extensions.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "bd_device.cuh"
@@ -65,6 +66,10 @@ struct mr_x_args {
     int L, upper;
     int My, Mz, cmx, cmy, cmz;
     mr_kernel_ref K;
+    int *status;         // device status word of the plan (MR_DEV_ERR_*), or NULL
+    // TMA tensor map of the source rows (pass 3 loads its tile with it),
+    // encoded by the launcher
+    CUtensorMap in_map;
 };
 
 int mr_launch_strided(int dir, int lmode, int smode, const mr_strided_args &a,
@@ -142,6 +147,10 @@ int mr_plan_group(mr_aha_plan plan);
 cudaStream_t mr_plan_stream(mr_aha_plan plan);
 // Number of kernels one execute launches (for accounting).
 int mr_plan_launch_count(mr_aha_plan plan);
+// Reads and clears the plan's device status word (0, or an MR_DEV_ERR_* code
+// a kernel recorded, e.g. a bounded wait that ran out); synchronises the
+// plan's stream.
+int mr_plan_device_status(mr_aha_plan plan, int *status);
 
 // Plan over caller-provided device scratch: fills `storage` (at least
 // mr_plan_struct_size() bytes, host memory) with a plan whose work buffers

@@ -637,6 +637,18 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     return MR_SUCCESS;
 }
 
+extern "C" int mr_b200_op_device_status(mr_op op, int *status) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && status != nullptr, "mr_b200_op_device_status: NULL argument");
+    *status = 0;
+    if (!op->plan) return MR_SUCCESS;
+    int prev = -1;
+    int rc = mr_push_device(&op->cfg, &prev);
+    if (rc == MR_SUCCESS) rc = mr_plan_device_status(op->plan, status);
+    mr_pop_device(prev);
+    return rc;
+}
+
 extern "C" int mr_b200_op_launches(mr_op op, int *n) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && n != nullptr, "mr_b200_op_launches: NULL argument");

@@ -6,6 +6,7 @@
 
 #include "engine.h"
 #include "fftfix.cuh"
+#include "tma.cuh"
 
 namespace {
 
@@ -208,10 +209,14 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__
 // transforms of half-empty ones. Row b = (coil, rank) of the tile keeps its
 // even half-spectrum in line 2b and its odd one in line 2b + 1. BLK: read
 // the complex64 kernel from its blocked copy (a.K.blk, unmasked only), where
-// the 32 frequencies of a warp are contiguous for every component.
-template <int N, int L, int NC, int KF, int kNT, bool BLK = false>
+// the 32 frequencies of a warp are contiguous for every component. TMAIN:
+// the CTA's NC L input rows arrive by TMA tensor copies (a.in_map: extents
+// {N, plane_rows, planes of the group}, box {N or N / 2, 1, NC L}; planes
+// past the group read as zeros) into a staging area at the end of the line
+// buffer, instead of per-thread loads; same values, same arithmetic.
+template <int N, int L, int NC, int KF, int kNT, bool BLK = false, bool TMAIN = false>
 __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__ mr_x_args a) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(128) float2 sm[];
     constexpr int LS = odd_stride<N>();
     constexpr int NR = NC * L;
     constexpr int NL = 2 * NR;
@@ -224,16 +229,58 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
     const int nrow = ncoils * L;
     const int64_t pbase = (int64_t)c0 * L;
     const float2 *tw = a.ax.tw;  // W_M^e, e < M
-    const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
-    const int64_t rstride = a.plane_rows * a.s_row;
+    if constexpr (TMAIN) {
+        constexpr int BX = N > 256 ? N / 2 : N;
+        constexpr int NBOX = N / BX;
+        constexpr int SOFF = ((NL * LS - NR * N) / 16) * 16;  // 128-byte aligned staging
+        constexpr int PER = (NR * N + kNT - 1) / kNT;
+        static_assert(N % BX == 0 && BX <= 256 && NR <= 256 && SOFF >= 0, "TMA box");
+        float2 *stage = sm + SOFF;
+        uint64_t *bar = reinterpret_cast<uint64_t *>(sm + NL * LS);
+        if (threadIdx.x == 0) {
+            mrtma::mbar_init(bar, 1);
+            mrtma::fence_mbar_init();
+            mrtma::mbar_arrive_expect_tx(bar, NR * N * (unsigned)sizeof(float2));
+#pragma unroll
+            for (int q = 0; q < NBOX; ++q)
+                mrtma::tensor3d_g2s(stage + q * NR * BX, &a.in_map, q * BX, loc, (int)pbase, bar);
+        }
+        __syncthreads();
+        mrtma::mbar_wait(bar, 0, a.status);
+        float2 vals[PER];
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int idx = threadIdx.x + k * kNT;
+            if (idx < NR * N) {
+                const int b = idx / N;
+                const int n = idx - b * N;
+                const int q = n / BX;
+                vals[k] = stage[(q * NR + b) * BX + (n - q * BX)];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; ++k) {
+            const int idx = threadIdx.x + k * kNT;
+            if (idx < NR * N) {
+                const int b = idx / N;
+                const int n = idx - b * N;
+                sm[(2 * b) * LS + n] = vals[k];
+                sm[(2 * b + 1) * LS + n] = c_mul(vals[k], __ldg(tw + n));
+            }
+        }
+    } else {
+        const float2 *src = a.src + (pbase * a.plane_rows + loc) * a.s_row;
+        const int64_t rstride = a.plane_rows * a.s_row;
 #pragma unroll 4
-    for (int idx = threadIdx.x; idx < NR * N; idx += kNT) {
-        const int b = idx / N;
-        const int n = idx - b * N;
-        float2 v = make_float2(0.f, 0.f);
-        if (b < nrow) v = src[b * rstride + n];
-        sm[(2 * b) * LS + n] = v;
-        sm[(2 * b + 1) * LS + n] = c_mul(v, __ldg(tw + n));
+        for (int idx = threadIdx.x; idx < NR * N; idx += kNT) {
+            const int b = idx / N;
+            const int n = idx - b * N;
+            float2 v = make_float2(0.f, 0.f);
+            if (b < nrow) v = src[b * rstride + n];
+            sm[(2 * b) * LS + n] = v;
+            sm[(2 * b + 1) * LS + n] = c_mul(v, __ldg(tw + n));
+        }
     }
     __syncthreads();
     mrfix::fft<-1, N, NL, 1, LS, kNT, 2>(sm, tw);
@@ -850,6 +897,24 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
     if constexpr (KF == MR_KF_F32) {
         if (a.K.blk && !a.K.inv) {
+            if (mr_env_int("MR_AHA_B200_NO_TMA", 0) == 0 && ((uintptr_t)a.src & 15) == 0 &&
+                (a.s_row & 1) == 0 && a.plane_rows <= 0x7fffffff) {
+                // the group's rows as a 3-D tensor {x, row of a plane, plane}
+                mr_x_args b = a;
+                const uint64_t dim[3] = {(uint64_t)N, (uint64_t)a.plane_rows,
+                                         (uint64_t)a.ncoil * L};
+                const uint64_t str[2] = {(uint64_t)a.s_row * sizeof(float2),
+                                         (uint64_t)a.plane_rows * a.s_row * sizeof(float2)};
+                const uint32_t box[3] = {(uint32_t)(N > 256 ? N / 2 : N), 1u, (uint32_t)(NC * L)};
+                const int rc = mr_tma_encode_3d(&b.in_map, a.src, dim, str, box);
+                if (rc != MR_SUCCESS) return rc;
+                static unsigned long long attr_t = 0;
+                set_attr(k_xbdh<N, L, NC, KF, kNT, true, true>, attr_t);
+                k_xbdh<N, L, NC, KF, kNT, true, true><<<(unsigned)nblk, kNT, smem + 16, s>>>(b);
+                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked,tma>", N, L,
+                                  NC, kNT);
+                return MR_SUCCESS;
+            }
             static unsigned long long attr_b = 0;
             set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
             k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);

@@ -9,8 +9,10 @@ instantiation ran each pass; every test asserts the headline ones:
   (56-point z lines, radix 8 x 7);
 * pass 2 ``k_hf_pipe<N=320,XT=8>`` and pass 4 ``k_strided_hi<N=320,XT=16>``
   (half-length 320-point y lines);
-* pass 3 ``k_xbdh<N=320,L=16,NC=1,F32,256,blocked>`` (half-length x lines and
-  the packed 16 x 16 Hermitian block multiply).
+* pass 3 ``k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>`` (half-length x lines
+  and the packed 16 x 16 Hermitian block multiply, input rows loaded by TMA
+  tensor copies); with ``MR_AHA_B200_NO_TMA=1`` the same kernel with
+  per-thread loads, bit-identical.
 
 Checks, relative L2 (tolerances written in each test):
 
@@ -50,7 +52,8 @@ REF_LIB = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "libmr_ah
 
 Z_KERNELS = ("k_xs_pipe<M=56,XT=32>", "k_coilsum_pipe<M=56,XT=32>")
 XY_KERNELS = ("k_hf_pipe<N=320,XT=8>", "k_strided_hi<N=320,XT=16>")
-X_BLOCKED = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked>"
+X_BLOCKED = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>"
+X_BLOCKED_REGS = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked>"
 X_PLAIN = "k_xbdh<N=320,L=16,NC=1,F32,256>"
 
 
@@ -108,14 +111,20 @@ def slab():
     op.close()
 
 
-def test_slab320_blocked_and_reference_layout_vs_fp64(slab):
+def test_slab320_blocked_and_reference_layout_vs_fp64(slab, monkeypatch):
     p, op, K, ref = slab
     assert op.blocked_copy(True) is True
     y, trace = traced(lambda: host(op(dev(p["x"]))))
     assert X_BLOCKED in trace and all(k in trace for k in XY_KERNELS), trace
+    assert op.device_status == 0
     err = O.rel_l2(y, ref)
     print(f"slab320 blocked copy vs FP64: {err:.3e}")
     assert err <= 1e-5, err
+    monkeypatch.setenv("MR_AHA_B200_NO_TMA", "1")
+    y1, trace1 = traced(lambda: host(op(dev(p["x"]))))
+    monkeypatch.delenv("MR_AHA_B200_NO_TMA")
+    assert X_BLOCKED_REGS in trace1, trace1
+    np.testing.assert_array_equal(y1, y)
     assert op.blocked_copy(False) is False
     y2, trace2 = traced(lambda: host(op(dev(p["x"]))))
     assert X_PLAIN in trace2 and X_BLOCKED not in trace2, trace2
@@ -191,6 +200,7 @@ def test_stack320_vs_reference_cuda_apply():
         y, trace = traced(lambda: op(x))
         for k in Z_KERNELS + XY_KERNELS + (X_BLOCKED,):
             assert k in trace, trace
+        assert op.device_status == 0
         # the reference's own apply of the same kernel
         rcfg = MRConfig.from_buffer_copy(cfg)
         plan = ctypes.c_void_p()
