@@ -461,6 +461,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         if (has_z) {
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
+            a.status = p->d_status;
             // z lines: the (y, x) plane is contiguous, so tiles run over the
             // flattened plane index
             a.ax = p->ax[2];
@@ -492,6 +493,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         {
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
+            a.status = p->d_status;
             a.ax = p->ax[1];
             a.nfast = Nx;
             a.xt = p->xt_y;
@@ -617,6 +619,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         {
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
+            a.status = p->d_status;
             a.ax = p->ax[1];
             a.nfast = Nx;
             a.xt = p->xt_y;
@@ -667,6 +670,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         if (has_z) {
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
+            a.status = p->d_status;
             a.ax = p->ax[2];
             a.nfast = Nx * Ny;
             a.nouter = 1;

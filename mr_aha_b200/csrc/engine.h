@@ -42,6 +42,10 @@ struct mr_strided_args {
     int n_out, shift_out;
     int ncoil, accumulate;
     float scale;
+    int *status;         // device status word of the plan (MR_DEV_ERR_*), or NULL
+    // TMA tensor maps of the pipelined z passes' tiles (encoded by the
+    // launcher): map0 the image / input planes, map1 the coil maps
+    CUtensorMap map0, map1;
 };
 
 // Lines along the contiguous axis (rows). Plain mode: rows r of src (stride

@@ -692,9 +692,12 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
 // other half of a double buffer (cp.async), so the loads overlap the FFT
 // instead of stalling it. Same arithmetic and order as k_strided3<1, BUF,
 // COILSUM>. Shared memory: input and map tiles x 2 stages, FFT buffer, sum.
-template <int M, int XT, int kNT, int MINB>
+// TMA: each tile is one tensor copy (a.map0: input planes {fast, z, plane},
+// a.map1: coil maps {fast, z, coil}; columns past the plane read as zeros)
+// completing on the stage's mbarrier, instead of per-thread cp.async.
+template <int M, int XT, int kNT, int MINB, bool TMA = false>
 __global__ void __launch_bounds__(kNT, MINB) k_coilsum_pipe(const __grid_constant__ mr_strided_args a) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(128) float2 sm[];
     constexpr int TILE = M * XT;
     float2 *wst = sm;                 // [2][M][XT] input tiles
     float2 *sst = sm + 2 * TILE;      // [2][M][XT] coil-map tiles (n_out rows used)
@@ -709,21 +712,41 @@ __global__ void __launch_bounds__(kNT, MINB) k_coilsum_pipe(const __grid_constan
     const int nx = min(XT, a.nfast - x0);
     const int64_t off0 = (int64_t)outer * a.s_outer + x0;
     const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 6 * TILE);  // TMA: one per stage
     auto issue = [&](int cc, int st) {
-        const float2 *srcp = a.src + (int64_t)(cc * a.L + plane) * a.s_plane + off0;
-        mr_cp_tile<XT, kNT>(wst + st * TILE, srcp, a.s_axis, a.n_in, nx);
-        const float2 *sp = a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0;
-        mr_cp_tile<XT, kNT>(sst + st * TILE, sp, a.d_axis, a.n_out, nx);
-        mr_cp_async_commit();
+        if constexpr (TMA) {
+            if (threadIdx.x == 0) {
+                mrtma::fence_proxy_async_smem();
+                mrtma::mbar_arrive_expect_tx(bar + st, (a.n_in + a.n_out) * XT *
+                                                           (unsigned)sizeof(float2));
+                mrtma::tensor3d_g2s(wst + st * TILE, &a.map0, x0, 0, cc * a.L + plane, bar + st);
+                mrtma::tensor3d_g2s(sst + st * TILE, &a.map1, x0, 0, a.coil0 + cc, bar + st);
+            }
+        } else {
+            const float2 *srcp = a.src + (int64_t)(cc * a.L + plane) * a.s_plane + off0;
+            mr_cp_tile<XT, kNT>(wst + st * TILE, srcp, a.s_axis, a.n_in, nx);
+            const float2 *sp = a.xs_s + (int64_t)(a.coil0 + cc) * a.img_plane + doff0;
+            mr_cp_tile<XT, kNT>(sst + st * TILE, sp, a.d_axis, a.n_out, nx);
+            mr_cp_async_commit();
+        }
     };
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            mrtma::mbar_init(bar, 1);
+            mrtma::mbar_init(bar + 1, 1);
+            mrtma::fence_mbar_init();
+        }
+        __syncthreads();
+    }
     issue(0, 0);
     for (int cc = 0; cc < a.ncoil; ++cc) {
         const int st = cc & 1;
-        if (cc + 1 < a.ncoil) {
-            issue(cc + 1, st ^ 1);
-            mr_cp_async_wait<1>();
+        if (cc + 1 < a.ncoil) issue(cc + 1, st ^ 1);
+        if constexpr (TMA) {
+            mrtma::mbar_wait(bar + st, (unsigned)(cc >> 1) & 1u, a.status);
         } else {
-            mr_cp_async_wait<0>();
+            if (cc + 1 < a.ncoil) mr_cp_async_wait<1>();
+            else mr_cp_async_wait<0>();
         }
         __syncthreads();
         const float2 *w = wst + st * TILE;
@@ -760,10 +783,13 @@ __global__ void __launch_bounds__(kNT, MINB) k_coilsum_pipe(const __grid_constan
 // over the ranks: a CTA takes one coil's L planes of a tile; the coil-map
 // tile is copied once, and the next rank's image tile is copied (cp.async)
 // while the current one is transformed. Same arithmetic as k_strided3<-1,
-// XS, BUF> (S_c x_l, then the FFT), so the results are identical.
-template <int M, int XT, int kNT, int MINB>
+// XS, BUF> (S_c x_l, then the FFT), so the results are identical. TMA: each
+// tile is one tensor copy (a.map0: image planes {fast, z, rank}, a.map1:
+// coil maps {fast, z, coil}; columns past the plane read as zeros)
+// completing on an mbarrier, instead of per-thread cp.async.
+template <int M, int XT, int kNT, int MINB, bool TMA = false>
 __global__ void __launch_bounds__(kNT, MINB) k_xs_pipe(const __grid_constant__ mr_strided_args a) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(128) float2 sm[];
     constexpr int TILE = M * XT;
     float2 *sst = sm;                // coil-map tile (n_in rows)
     float2 *xst = sm + TILE;         // [2] image tiles
@@ -778,19 +804,46 @@ __global__ void __launch_bounds__(kNT, MINB) k_xs_pipe(const __grid_constant__ m
     const int nx = min(XT, a.nfast - x0);
     const int64_t off0 = (int64_t)outer * a.s_outer + x0;
     const int64_t doff0 = (int64_t)outer * a.d_outer + x0;
-    mr_cp_tile<XT, kNT>(sst, a.xs_s + (int64_t)(a.coil0 + cg) * a.img_plane + off0, a.s_axis,
-                        a.n_in, nx);
-    mr_cp_tile<XT, kNT>(xst, a.xs_x + off0, a.s_axis, a.n_in, nx);
-    mr_cp_async_commit();
+    // TMA: bar[0] the coil-map tile, bar[1 + st] the image tile of stage st
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 4 * TILE);
+    const unsigned tb = a.n_in * XT * (unsigned)sizeof(float2);
+    if constexpr (TMA) {
+        if (threadIdx.x == 0) {
+            for (int q = 0; q < 3; ++q) mrtma::mbar_init(bar + q, 1);
+            mrtma::fence_mbar_init();
+            mrtma::mbar_arrive_expect_tx(bar, tb);
+            mrtma::tensor3d_g2s(sst, &a.map1, x0, 0, a.coil0 + cg, bar);
+            mrtma::mbar_arrive_expect_tx(bar + 1, tb);
+            mrtma::tensor3d_g2s(xst, &a.map0, x0, 0, 0, bar + 1);
+        }
+        __syncthreads();
+        mrtma::mbar_wait(bar, 0, a.status);
+    } else {
+        mr_cp_tile<XT, kNT>(sst, a.xs_s + (int64_t)(a.coil0 + cg) * a.img_plane + off0, a.s_axis,
+                            a.n_in, nx);
+        mr_cp_tile<XT, kNT>(xst, a.xs_x + off0, a.s_axis, a.n_in, nx);
+        mr_cp_async_commit();
+    }
     for (int l = 0; l < a.L; ++l) {
         const int st = l & 1;
-        if (l + 1 < a.L) {
-            mr_cp_tile<XT, kNT>(xst + (st ^ 1) * TILE, a.xs_x + (int64_t)(l + 1) * a.img_plane + off0,
-                                a.s_axis, a.n_in, nx);
-            mr_cp_async_commit();
-            mr_cp_async_wait<1>();
+        if constexpr (TMA) {
+            if (l + 1 < a.L && threadIdx.x == 0) {
+                mrtma::fence_proxy_async_smem();
+                mrtma::mbar_arrive_expect_tx(bar + 1 + (st ^ 1), tb);
+                mrtma::tensor3d_g2s(xst + (st ^ 1) * TILE, &a.map0, x0, 0, l + 1,
+                                    bar + 1 + (st ^ 1));
+            }
+            mrtma::mbar_wait(bar + 1 + st, (unsigned)(l >> 1) & 1u, a.status);
         } else {
-            mr_cp_async_wait<0>();
+            if (l + 1 < a.L) {
+                mr_cp_tile<XT, kNT>(xst + (st ^ 1) * TILE,
+                                    a.xs_x + (int64_t)(l + 1) * a.img_plane + off0, a.s_axis,
+                                    a.n_in, nx);
+                mr_cp_async_commit();
+                mr_cp_async_wait<1>();
+            } else {
+                mr_cp_async_wait<0>();
+            }
         }
         __syncthreads();
         const float2 *xv = xst + st * TILE;
@@ -817,6 +870,14 @@ inline bool mr_xs_pipe_ok(const mr_strided_args &a) {
            a.nplane % a.L == 0;
 }
 
+// Whether a pipelined z pass may load its tiles by TMA: one outer block (the
+// tiles are boxes of 3-D tensors {fast, z, plane}), lines of at most 256
+// points (the box limit), not switched off (MR_AHA_B200_NO_TMA).
+inline bool mr_tma_tiles_ok(const mr_strided_args &a) {
+    return mr_env_int("MR_AHA_B200_NO_TMA", 0) == 0 && a.nouter == 1 && a.n_in <= 256 &&
+           a.nfast >= 1;
+}
+
 // Whether the pipelined coil-sum pass can take these arguments: 16-byte
 // aligned tiles (even strides and offsets, aligned bases).
 inline bool mr_coilsum_pipe_ok(const mr_strided_args &a) {
@@ -836,11 +897,32 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
                   mrfix::factor(M).n >= 2 && 4 * M * XT * 8 <= 112 * 1024) {
         if (mr_xs_pipe_ok(a)) {
             constexpr int PB = (4 * M * XT * 8 <= 48 * 1024) ? 4 : 2;
-            static unsigned long long attr_x = 0;
-            set_attr(k_xs_pipe<M, XT, 256, PB>, attr_x);
             const int64_t nb = (int64_t)a.nxt * a.nouter * (a.nplane / a.L);
             if (nb <= 0) return MR_SUCCESS;
             if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+            if constexpr ((M * XT) % 16 == 0 && M <= 256 && XT <= 256) {
+                if (mr_tma_tiles_ok(a)) {
+                    // image planes {fast, z, rank} and coil maps {fast, z, coil}
+                    mr_strided_args b = a;
+                    const uint64_t d0[3] = {(uint64_t)a.nfast, (uint64_t)a.n_in, (uint64_t)a.L};
+                    const uint64_t d1[3] = {(uint64_t)a.nfast, (uint64_t)a.n_in,
+                                            (uint64_t)(a.coil0 + a.nplane / a.L)};
+                    const uint64_t st[2] = {(uint64_t)a.s_axis * sizeof(float2),
+                                            (uint64_t)a.img_plane * sizeof(float2)};
+                    const uint32_t box[3] = {(uint32_t)XT, (uint32_t)a.n_in, 1u};
+                    int rc = mr_tma_encode_3d(&b.map0, a.xs_x, d0, st, box);
+                    if (rc == MR_SUCCESS) rc = mr_tma_encode_3d(&b.map1, a.xs_s, d1, st, box);
+                    if (rc != MR_SUCCESS) return rc;
+                    static unsigned long long attr_t = 0;
+                    set_attr(k_xs_pipe<M, XT, 256, PB, true>, attr_t);
+                    k_xs_pipe<M, XT, 256, PB, true>
+                        <<<(unsigned)nb, 256, (size_t)4 * M * XT * sizeof(float2) + 32, s>>>(b);
+                    MR_LAUNCH_CHECK_T("k_xs_pipe", "k_xs_pipe<M=%d,XT=%d,tma>", M, XT);
+                    return MR_SUCCESS;
+                }
+            }
+            static unsigned long long attr_x = 0;
+            set_attr(k_xs_pipe<M, XT, 256, PB>, attr_x);
             k_xs_pipe<M, XT, 256, PB><<<(unsigned)nb, 256, (size_t)4 * M * XT * sizeof(float2),
                                         s>>>(a);
             MR_LAUNCH_CHECK_T("k_xs_pipe", "k_xs_pipe<M=%d,XT=%d>", M, XT);
@@ -852,11 +934,36 @@ int launch_s3(const mr_strided_args &a, cudaStream_t s) {
         if (mr_coilsum_pipe_ok(a)) {
             // CTAs per SM that the shared memory allows, at most 4
             constexpr int PB = (6 * M * XT * 8 <= 48 * 1024) ? 4 : 2;
-            static unsigned long long attr_p = 0;
-            set_attr(k_coilsum_pipe<M, XT, 256, PB>, attr_p);
             const int64_t nb = (int64_t)a.nxt * a.nouter * a.nplane;
             if (nb <= 0) return MR_SUCCESS;
             if (nb > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "strided pass grid too large");
+            if constexpr ((M * XT) % 16 == 0 && M <= 256 && XT <= 256) {
+                if (mr_tma_tiles_ok(a) && a.n_out <= 256) {
+                    // input planes {fast, z, plane} and coil maps {fast, z, coil}
+                    mr_strided_args b = a;
+                    const uint64_t d0[3] = {(uint64_t)a.nfast, (uint64_t)a.n_in,
+                                            (uint64_t)a.ncoil * a.L};
+                    const uint64_t s0[2] = {(uint64_t)a.s_axis * sizeof(float2),
+                                            (uint64_t)a.s_plane * sizeof(float2)};
+                    const uint32_t b0[3] = {(uint32_t)XT, (uint32_t)a.n_in, 1u};
+                    const uint64_t d1[3] = {(uint64_t)a.nfast, (uint64_t)a.n_out,
+                                            (uint64_t)(a.coil0 + a.ncoil)};
+                    const uint64_t s1[2] = {(uint64_t)a.d_axis * sizeof(float2),
+                                            (uint64_t)a.img_plane * sizeof(float2)};
+                    const uint32_t b1[3] = {(uint32_t)XT, (uint32_t)a.n_out, 1u};
+                    int rc = mr_tma_encode_3d(&b.map0, a.src, d0, s0, b0);
+                    if (rc == MR_SUCCESS) rc = mr_tma_encode_3d(&b.map1, a.xs_s, d1, s1, b1);
+                    if (rc != MR_SUCCESS) return rc;
+                    static unsigned long long attr_t = 0;
+                    set_attr(k_coilsum_pipe<M, XT, 256, PB, true>, attr_t);
+                    k_coilsum_pipe<M, XT, 256, PB, true>
+                        <<<(unsigned)nb, 256, (size_t)6 * M * XT * sizeof(float2) + 32, s>>>(b);
+                    MR_LAUNCH_CHECK_T("k_coilsum_pipe", "k_coilsum_pipe<M=%d,XT=%d,tma>", M, XT);
+                    return MR_SUCCESS;
+                }
+            }
+            static unsigned long long attr_p = 0;
+            set_attr(k_coilsum_pipe<M, XT, 256, PB>, attr_p);
             k_coilsum_pipe<M, XT, 256, PB><<<(unsigned)nb, 256,
                                              (size_t)6 * M * XT * sizeof(float2), s>>>(a);
             MR_LAUNCH_CHECK_T("k_coilsum_pipe", "k_coilsum_pipe<M=%d,XT=%d>", M, XT);

@@ -5,8 +5,10 @@ kernel, so pass 3 reads the blocked kernel copy).
 The launch trace (``mr_b200_trace_launches``) shows which template
 instantiation ran each pass; every test asserts the headline ones:
 
-* pass 1 ``k_xs_pipe<M=56,XT=32>`` and pass 5 ``k_coilsum_pipe<M=56,XT=32>``
-  (56-point z lines, radix 8 x 7);
+* pass 1 ``k_xs_pipe<M=56,XT=32,tma>`` and pass 5
+  ``k_coilsum_pipe<M=56,XT=32,tma>`` (56-point z lines, radix 8 x 7, tiles
+  loaded by TMA tensor copies; with ``MR_AHA_B200_NO_TMA=1`` by per-thread
+  cp.async, bit-identical);
 * pass 2 ``k_hf_pipe<N=320,XT=8>`` and pass 4 ``k_strided_hi<N=320,XT=16>``
   (half-length 320-point y lines);
 * pass 3 ``k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>`` (half-length x lines
@@ -50,7 +52,7 @@ pytestmark = pytest.mark.gpu
 
 REF_LIB = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "libmr_aha_ref.so"
 
-Z_KERNELS = ("k_xs_pipe<M=56,XT=32>", "k_coilsum_pipe<M=56,XT=32>")
+Z_KERNELS = ("k_xs_pipe<M=56,XT=32,tma>", "k_coilsum_pipe<M=56,XT=32,tma>")
 XY_KERNELS = ("k_hf_pipe<N=320,XT=8>", "k_strided_hi<N=320,XT=16>")
 X_BLOCKED = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>"
 X_BLOCKED_REGS = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked>"
@@ -83,16 +85,22 @@ def _oracle(p, K, upper=False):
                                p["SEs"], K, upper=upper)
 
 
-def test_z56_kernels_vs_fp64():
+def test_z56_kernels_vs_fp64(monkeypatch):
     import mr_aha_b200 as mr
 
     p = synth.spec_inputs(_spec((64, 64, 56), 16, 12, 48, seed=21))
     cfg = mr.make_config("stack", p["n_dim"], p["L"], n_coils=p["n_coils"])
     with mr.create_op(cfg, dev(p["SEs"]), dev(p["phi2"]), dev(p["traj"])) as op:
         y, trace = traced(lambda: host(op(dev(p["x"]))))
+        assert op.device_status == 0
+        monkeypatch.setenv("MR_AHA_B200_NO_TMA", "1")
+        y_cp, trace_cp = traced(lambda: host(op(dev(p["x"]))))
+        monkeypatch.delenv("MR_AHA_B200_NO_TMA")
         K = host(op.kernel())
     for k in Z_KERNELS:
         assert k in trace, trace
+        assert k.replace(",tma>", ">") in trace_cp, trace_cp
+    np.testing.assert_array_equal(y_cp, y)
     err = O.rel_l2(y, _oracle(p, K))
     print(f"z56 (64x64x56, L=16, 12 coils) vs FP64: {err:.3e}")
     assert err <= 1e-5, err
