@@ -529,9 +529,12 @@ __global__ void __launch_bounds__(kNT, MINB) k_strided_hi(const __grid_constant_
 // (cp.async) into the other stage while the current plane is transformed.
 // The first FFT pass reads the stage (the odd line times t[n]), the last one
 // writes the spectrum rows. Same arithmetic as k_strided_hf.
-template <int N, int XT, int kNT, int MINB, int PG>
+// TMA: each plane's [N][XT] tile arrives as tensor copies of boxes of at
+// most 256 rows (a.map0: {fast, y, outer, plane}; columns past the plane read
+// as zeros) completing on the stage's mbarrier, instead of per-thread cp.async.
+template <int N, int XT, int kNT, int MINB, int PG, bool TMA = false>
 __global__ void __launch_bounds__(kNT, MINB) k_hf_pipe(const __grid_constant__ mr_strided_args a) {
-    extern __shared__ float2 sm[];
+    extern __shared__ __align__(128) float2 sm[];
     constexpr int NL = 2 * XT;
     constexpr int STG = N * XT;
     float2 *stg = sm;               // [2][N][XT]
@@ -549,17 +552,42 @@ __global__ void __launch_bounds__(kNT, MINB) k_hf_pipe(const __grid_constant__ m
     const int64_t soff = (int64_t)outer * a.s_outer + x0;
     const int64_t doff = (int64_t)outer * a.d_outer + x0;
     const float2 *tw = a.ax.tw;
-    mr_cp_tile<XT, kNT>(stg, a.src + (int64_t)p0 * a.s_plane + soff, a.s_axis, N, nx);
-    mr_cp_async_commit();
+    constexpr int BY = N > 256 ? N / 2 : N;  // rows per tensor box
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + 2 * STG + N * NL);
+    auto issue = [&](int pl, int st) {
+        if constexpr (TMA) {
+            if (threadIdx.x == 0) {
+                mrtma::fence_proxy_async_smem();
+                mrtma::mbar_arrive_expect_tx(bar + st, N * XT * (unsigned)sizeof(float2));
+#pragma unroll
+                for (int q = 0; q < N / BY; ++q)
+                    mrtma::tensor4d_g2s(stg + st * STG + q * BY * XT, &a.map0, x0, q * BY, outer,
+                                        pl, bar + st);
+            }
+        } else {
+            mr_cp_tile<XT, kNT>(stg + st * STG, a.src + (int64_t)pl * a.s_plane + soff, a.s_axis,
+                                N, nx);
+            mr_cp_async_commit();
+        }
+    };
+    if constexpr (TMA) {
+        static_assert(N % BY == 0 && BY <= 256 && XT <= 256, "TMA box");
+        if (threadIdx.x == 0) {
+            mrtma::mbar_init(bar, 1);
+            mrtma::mbar_init(bar + 1, 1);
+            mrtma::fence_mbar_init();
+        }
+        __syncthreads();
+    }
+    issue(p0, 0);
     for (int i = 0; i < np; ++i) {
         const int st = i & 1;
-        if (i + 1 < np) {
-            mr_cp_tile<XT, kNT>(stg + (st ^ 1) * STG, a.src + (int64_t)(p0 + i + 1) * a.s_plane + soff,
-                                a.s_axis, N, nx);
-            mr_cp_async_commit();
-            mr_cp_async_wait<1>();
+        if (i + 1 < np) issue(p0 + i + 1, st ^ 1);
+        if constexpr (TMA) {
+            mrtma::mbar_wait(bar + st, (unsigned)(i >> 1) & 1u, a.status);
         } else {
-            mr_cp_async_wait<0>();
+            if (i + 1 < np) mr_cp_async_wait<1>();
+            else mr_cp_async_wait<0>();
         }
         __syncthreads();
         const float2 *sv = stg + st * STG;
@@ -652,9 +680,27 @@ int launch_sh(const mr_strided_args &a, cudaStream_t s) {
         constexpr int PG = 8;
         if (mr_env_int("MR_AHA_B200_NO_PIPE", 0) == 0 && (((uintptr_t)a.src) & 15) == 0 &&
             ((a.s_plane | a.s_axis | a.s_outer) & 1) == 0) {
+            const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
+            if (mr_env_int("MR_AHA_B200_NO_TMA", 0) == 0 && N / (N > 256 ? 2 : 1) <= 256) {
+                // planes {x, y, z (outer), plane}
+                mr_strided_args b = a;
+                const uint64_t dim[4] = {(uint64_t)a.nfast, (uint64_t)N, (uint64_t)a.nouter,
+                                         (uint64_t)a.nplane};
+                const uint64_t str[3] = {(uint64_t)a.s_axis * sizeof(float2),
+                                         (uint64_t)a.s_outer * sizeof(float2),
+                                         (uint64_t)a.s_plane * sizeof(float2)};
+                const uint32_t box[4] = {(uint32_t)XT, (uint32_t)(N > 256 ? N / 2 : N), 1u, 1u};
+                const int rc = mr_tma_encode(&b.map0, a.src, 4, dim, str, box);
+                if (rc != MR_SUCCESS) return rc;
+                static unsigned long long attr_t = 0;
+                set_attr(k_hf_pipe<N, XT, kNT, 2, PG, true>, attr_t);
+                k_hf_pipe<N, XT, kNT, 2, PG, true>
+                    <<<(unsigned)nb, kNT, (size_t)4 * N * XT * sizeof(float2) + 16, s>>>(b);
+                MR_LAUNCH_CHECK_T("k_hf_pipe", "k_hf_pipe<N=%d,XT=%d,tma>", N, XT);
+                return MR_SUCCESS;
+            }
             static unsigned long long attr_p = 0;
             set_attr(k_hf_pipe<N, XT, kNT, 2, PG>, attr_p);
-            const int64_t nb = (int64_t)a.nxt * a.nouter * ((a.nplane + PG - 1) / PG);
             k_hf_pipe<N, XT, kNT, 2, PG><<<(unsigned)nb, kNT, (size_t)4 * N * XT * sizeof(float2),
                                            s>>>(a);
             MR_LAUNCH_CHECK_T("k_hf_pipe", "k_hf_pipe<N=%d,XT=%d>", N, XT);

@@ -9,8 +9,8 @@ instantiation ran each pass; every test asserts the headline ones:
   ``k_coilsum_pipe<M=56,XT=32,tma>`` (56-point z lines, radix 8 x 7, tiles
   loaded by TMA tensor copies; with ``MR_AHA_B200_NO_TMA=1`` by per-thread
   cp.async, bit-identical);
-* pass 2 ``k_hf_pipe<N=320,XT=8>`` and pass 4 ``k_strided_hi<N=320,XT=16>``
-  (half-length 320-point y lines);
+* pass 2 ``k_hf_pipe<N=320,XT=8,tma>`` (tiles loaded by TMA tensor copies)
+  and pass 4 ``k_strided_hi<N=320,XT=16>`` (half-length 320-point y lines);
 * pass 3 ``k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>`` (half-length x lines
   and the packed 16 x 16 Hermitian block multiply, input rows loaded by TMA
   tensor copies); with ``MR_AHA_B200_NO_TMA=1`` the same kernel with
@@ -53,7 +53,7 @@ pytestmark = pytest.mark.gpu
 REF_LIB = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "libmr_aha_ref.so"
 
 Z_KERNELS = ("k_xs_pipe<M=56,XT=32,tma>", "k_coilsum_pipe<M=56,XT=32,tma>")
-XY_KERNELS = ("k_hf_pipe<N=320,XT=8>", "k_strided_hi<N=320,XT=16>")
+XY_KERNELS = ("k_hf_pipe<N=320,XT=8,tma>", "k_strided_hi<N=320,XT=16>")
 X_BLOCKED = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>"
 X_BLOCKED_REGS = "k_xbdh<N=320,L=16,NC=1,F32,256,blocked>"
 X_PLAIN = "k_xbdh<N=320,L=16,NC=1,F32,256>"
