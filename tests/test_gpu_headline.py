@@ -10,7 +10,9 @@ instantiation ran each pass; every test asserts the headline ones:
   loaded by TMA tensor copies; with ``MR_AHA_B200_NO_TMA=1`` by per-thread
   cp.async, bit-identical);
 * pass 2 ``k_hf_pipe<N=320,XT=8,tma>`` (tiles loaded by TMA tensor copies)
-  and pass 4 ``k_strided_hi<N=320,XT=16>`` (half-length 320-point y lines);
+  and pass 4 ``k_strided_hi<N=320,XT=16>`` (first radix pass reading global
+  memory directly: a whole-tile TMA load ahead of it measured slower, 7.0
+  against 6.5 ms) -- half-length 320-point y lines;
 * pass 3 ``k_xbdh<N=320,L=16,NC=1,F32,256,blocked,tma>`` (half-length x lines
   and the packed 16 x 16 Hermitian block multiply, input rows loaded by TMA
   tensor copies); with ``MR_AHA_B200_NO_TMA=1`` the same kernel with
