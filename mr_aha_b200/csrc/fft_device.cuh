@@ -179,6 +179,68 @@ __device__ __forceinline__ void dft8(float2 *u) {
     u[1] = o[0]; u[3] = o[1]; u[5] = o[2]; u[7] = o[3];
 }
 
+// cos(2 pi m / R) and sin(2 pi m / R) for R = 16 or 20, from the cosines of
+// the first quadrant (cos(2 pi j / R), j = 0 .. R / 4) and the quadrant
+// symmetries, so that every value is the correctly rounded float of the
+// exact one.
+__host__ __device__ constexpr float quad_cos(int R, int j) {
+    constexpr double c16[5] = {1.0, 0.92387953251128675613, 0.70710678118654752440,
+                               0.38268343236508977173, 0.0};
+    constexpr double c20[6] = {1.0, 0.95105651629515357212, 0.80901699437494742410,
+                               0.58778525229247312917, 0.30901699437494742410, 0.0};
+    return (float)(R == 16 ? c16[j] : c20[j]);
+}
+__host__ __device__ constexpr float root_cos(int R, int m) {
+    const int q = (m % R) / (R / 4), r = (m % R) % (R / 4), Q = R / 4;
+    return q == 0 ? quad_cos(R, r) : q == 1 ? -quad_cos(R, Q - r)
+                                 : q == 2 ? -quad_cos(R, r) : quad_cos(R, Q - r);
+}
+__host__ __device__ constexpr float root_sin(int R, int m) {
+    const int q = (m % R) / (R / 4), r = (m % R) % (R / 4), Q = R / 4;
+    return q == 0 ? quad_cos(R, Q - r) : q == 1 ? quad_cos(R, r)
+                                     : q == 2 ? -quad_cos(R, Q - r) : -quad_cos(R, r);
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_small(float2 *u);
+
+// R = P Q point DFT in registers by one Cooley-Tukey step (n = Q n1 + n2,
+// k = k1 + P k2): X[k1 + P k2] = sum_{n2} W_Q^{n2 k2} W_R^{n2 k1}
+// sum_{n1} x[Q n1 + n2] W_P^{n1 k1}, W_R = exp(DIR 2 pi i / R); the inner
+// twiddles are compile-time constants (exact for multiples of pi / 2).
+template <int P, int Q, int DIR>
+__device__ __forceinline__ void dft_pq(float2 *u) {
+    constexpr int R = P * Q;
+    float2 a[Q][P];
+#pragma unroll
+    for (int n2 = 0; n2 < Q; ++n2) {
+#pragma unroll
+        for (int n1 = 0; n1 < P; ++n1) a[n2][n1] = u[Q * n1 + n2];
+        dft_small<P, DIR>(a[n2]);
+#pragma unroll
+        for (int k1 = 1; k1 < P; ++k1) {
+            const int m = (n2 * k1) % R;
+            if (m == 0) continue;
+            if (4 * m == R) a[n2][k1] = c_mul_i<DIR>(a[n2][k1]);
+            else if (2 * m == R) a[n2][k1] = make_float2(-a[n2][k1].x, -a[n2][k1].y);
+            else if (4 * m == 3 * R) a[n2][k1] = c_mul_i<-DIR>(a[n2][k1]);
+            else
+                a[n2][k1] = c_mul(a[n2][k1],
+                                  make_float2(root_cos(R, m), DIR < 0 ? -root_sin(R, m)
+                                                                      : root_sin(R, m)));
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < P; ++k1) {
+        float2 b[Q];
+#pragma unroll
+        for (int n2 = 0; n2 < Q; ++n2) b[n2] = a[n2][k1];
+        dft_small<Q, DIR>(b);
+#pragma unroll
+        for (int k2 = 0; k2 < Q; ++k2) u[k1 + P * k2] = b[k2];
+    }
+}
+
 template <int R, int DIR>
 __device__ __forceinline__ void dft_small(float2 *u) {
     if constexpr (R == 2) dft2<DIR>(u);
@@ -187,6 +249,8 @@ __device__ __forceinline__ void dft_small(float2 *u) {
     else if constexpr (R == 5) dft5<DIR>(u);
     else if constexpr (R == 7) dft7<DIR>(u);
     else if constexpr (R == 8) dft8<DIR>(u);
+    else if constexpr (R == 16) dft_pq<4, 4, DIR>(u);
+    else if constexpr (R == 20) dft_pq<4, 5, DIR>(u);
 }
 
 // ---- one Stockham pass over nlines lines ----------------------------------

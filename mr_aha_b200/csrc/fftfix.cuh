@@ -20,9 +20,21 @@ struct radix_list {
 
 // Radix policy of the host planner (passes.cu mr_fft_factor): eights, then a
 // four or a two, then fives, threes, sevens. Lengths with other factors are
-// not specialised (n = 0).
+// not specialised (n = 0). Exception: 320 (the half-length lines of the
+// 640-point grids) runs as 16 x 20, two register-resident passes instead of
+// three (8, 8, 5): one shared-memory round trip and barrier fewer per line.
+// Measured at 320 x 320 x 56, L = 16, 12 coils: y forward 6.51 -> 5.84 ms,
+// y inverse 6.52 -> 6.36 ms, x pass 3 (with its L2 kernel prefetch) 44.4 ->
+// 42.6 ms. Other lengths keep radix 8, whose smaller register stages spill
+// less.
 constexpr radix_list factor(int M) {
     radix_list l{0, {}};
+    if (M == 320) {
+        l.n = 2;
+        l.r[0] = 16;
+        l.r[1] = 20;
+        return l;
+    }
     int e2 = 0;
     while (M % 2 == 0) {
         M /= 2;
