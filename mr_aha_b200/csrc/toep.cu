@@ -110,7 +110,7 @@ struct gemm_args {
 };
 
 template <bool OUT_F32>
-__global__ void __launch_bounds__(256) k_zgemm(const gemm_args g) {
+__global__ void __launch_bounds__(256, 2) k_zgemm(const gemm_args g) {
     __shared__ double2 As[16][64 + 1];
     __shared__ double2 Bs[16][64 + 1];
     const int64_t batch = blockIdx.z;
