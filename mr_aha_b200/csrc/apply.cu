@@ -26,7 +26,10 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <nvtx3/nvToolsExt.h>
+
 #include <map>
 #include <mutex>
 #include <string>
@@ -415,7 +418,29 @@ static int launch_strided_auto(int dir, int lm, int sm, mr_strided_args a, int x
     return mr_launch_strided(dir, lm, sm, a, s);
 }
 
-static void prof_mark(mr_prof *prof, const char *name, cudaStream_t s) {
+// Host-side NVTX ranges of one execute ("mr_aha apply" > pass name, shown
+// in Nsight Systems timelines; NVTX calls return at once when no tool is
+// attached). Ranges still open at an early error return are closed on exit.
+struct nvtx_scope {
+    int depth = 0;
+    void push(const char *name) {
+        nvtxRangePushA(name);
+        ++depth;
+    }
+    void pop() {
+        if (depth > 0) {
+            nvtxRangePop();
+            --depth;
+        }
+    }
+    ~nvtx_scope() {
+        while (depth > 0) pop();
+    }
+};
+
+// End of a pass: an event for mr_b200_op_profile and the end of its range.
+static void prof_mark(mr_prof *prof, nvtx_scope &nv, const char *name, cudaStream_t s) {
+    nv.pop();
     if (!prof || prof->n >= MR_PROF_MAX) return;
     prof->name[prof->n] = name;
     cudaEventRecord(prof->ev[++prof->n], s);
@@ -436,7 +461,10 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
     mr_kernel_ref K = K0;
     int rc;
 
+    nvtx_scope nv;
+    nv.push("mr_aha apply");
     if (cfg.is_masked) {
+        nv.push("mask_inverse");
         const int64_t nm = cfg.num_masked;
         MR_CUDA_TRY(cudaMemsetAsync(p->d_inv, 0xFF, g.vpad * sizeof(int), s));
         k_mask_inverse<<<(unsigned)mr_cdiv(nm, 256), 256, 0, s>>>(p->d_inv, d_mask, nm, g);
@@ -444,7 +472,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         K.inv = p->d_inv;
         K.stride = nm;
         K.blk = nullptr;
-        prof_mark(prof, "mask_inverse", s);
+        prof_mark(prof, nv, "mask_inverse", s);
     } else {
         K.inv = nullptr;
         K.stride = g.vpad;
@@ -459,6 +487,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
 
         // ---- pass 1: z lines, S_c x_l, zero-pad along z ----
         if (has_z) {
+            nv.push("z_forward");
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
             a.status = p->d_status;
@@ -487,10 +516,11 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             rc = launch_strided_auto(-1, MR_LM_XS, MR_SM_BUF, a, p->xts_z_buf, p->xt_z, s,
                                      p->xt3_z_buf);
             if (rc != MR_SUCCESS) return rc;
-            prof_mark(prof, "z_forward", s);
+            prof_mark(prof, nv, "z_forward", s);
         }
         // ---- pass 2: y lines, zero-pad along y ----
         {
+            nv.push("y_forward");
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
             a.status = p->d_status;
@@ -534,7 +564,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                                          p->xt3_y_buf);
             }
             if (rc != MR_SUCCESS) return rc;
-            prof_mark(prof, "y_forward", s);
+            prof_mark(prof, nv, "y_forward", s);
         }
         // ---- pass 3: x lines with the block multiply ----
         {
@@ -543,6 +573,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             a.ax = p->ax[0];
             a.scale = 1.f;
             if (p->fused) {
+                nv.push("x_blockdiag");
                 a.src = p->W1;
                 a.dst = p->W1;
                 a.s_row = Nx;
@@ -583,8 +614,9 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                     rc = mr_launch_xbd(a, s);
                 }
                 if (rc != MR_SUCCESS) return rc;
-                prof_mark(prof, "x_blockdiag", s);
+                prof_mark(prof, nv, "x_blockdiag", s);
             } else {
+                nv.push("x_forward");
                 const int rows = 4;
                 a.rows_cta = rows;
                 a.src = p->W1;
@@ -598,10 +630,12 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.shift_out = 0;
                 rc = mr_launch_xplain(-1, a, s);
                 if (rc != MR_SUCCESS) return rc;
-                prof_mark(prof, "x_forward", s);
+                prof_mark(prof, nv, "x_forward", s);
+                nv.push("blockdiag");
                 rc = launch_bd_full(p->W2, p->W3, g, K, G, s);
                 if (rc != MR_SUCCESS) return rc;
-                prof_mark(prof, "blockdiag", s);
+                prof_mark(prof, nv, "blockdiag", s);
+                nv.push("x_inverse");
                 a.src = p->W3;
                 a.dst = p->W1;
                 a.s_row = Mx;
@@ -612,11 +646,12 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                 a.shift_out = g.cn[0];
                 rc = mr_launch_xplain(1, a, s);
                 if (rc != MR_SUCCESS) return rc;
-                prof_mark(prof, "x_inverse", s);
+                prof_mark(prof, nv, "x_inverse", s);
             }
         }
         // ---- pass 4: y lines back, crop ----
         {
+            nv.push("y_inverse");
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
             a.status = p->d_status;
@@ -664,10 +699,11 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
                                          p->xt3_y_cs);
             }
             if (rc != MR_SUCCESS) return rc;
-            prof_mark(prof, "y_inverse", s);
+            prof_mark(prof, nv, "y_inverse", s);
         }
         // ---- pass 5: z lines back, crop, conj(S_c) coil sum ----
         if (has_z) {
+            nv.push("z_inverse");
             mr_strided_args a;
             std::memset(&a, 0, sizeof(a));
             a.status = p->d_status;
@@ -697,7 +733,7 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
             rc = launch_strided_auto(1, MR_LM_BUF, MR_SM_COILSUM, a, p->xts_z_cs, p->xt_z, s,
                                      p->xt3_z_cs);
             if (rc != MR_SUCCESS) return rc;
-            prof_mark(prof, "z_inverse", s);
+            prof_mark(prof, nv, "z_inverse", s);
         }
     }
     if (cfg.verbose) {
@@ -902,14 +938,172 @@ static std::string tune_key(const mr_aha_plan p) {
     return b;
 }
 
+// Strided passes the autotuner sweeps: (xt3, xts) fields, axis length, store
+// mode, whether the plan runs that pass.
+struct mr_tune_knob {
+    int mr_tune_choice::*xt3;
+    int mr_tune_choice::*xts;
+    int M, smode;
+    bool on;
+};
+
+static void tune_knobs(const mr_aha_plan p, mr_tune_knob (&k)[5]) {
+    const mr_geom &g = p->g;
+    const bool has_z = p->cfg.n_spatial == 3;
+    k[0] = {&mr_tune_choice::xt3_z_buf, &mr_tune_choice::xts_z_buf, g.m[2], MR_SM_BUF, has_z};
+    k[1] = {&mr_tune_choice::xt3_y_buf, &mr_tune_choice::xts_y_buf, g.m[1], MR_SM_BUF, true};
+    k[2] = {&mr_tune_choice::xt3_yi, &mr_tune_choice::xts_yi, g.m[1], MR_SM_BUF, has_z};
+    k[3] = {&mr_tune_choice::xt3_y_cs, &mr_tune_choice::xts_y_cs, g.m[1], MR_SM_COILSUM, !has_z};
+    k[4] = {&mr_tune_choice::xt3_z_cs, &mr_tune_choice::xts_z_cs, g.m[2], MR_SM_COILSUM, has_z};
+}
+
+static bool tune_in(int v, const int *l, int n) {
+    for (int i = 0; i < n; ++i)
+        if (l[i] == v) return true;
+    return false;
+}
+
+// True when every field of c is a value the autotuner itself tries for this
+// plan, whose fields still hold their defaults: a cached choice from a file
+// is used only then, so a stale or edited line cannot select a kernel width
+// or coil group the plan has no launch for.
+static bool tune_valid(const mr_aha_plan p, const mr_tune_choice &c) {
+    const mr_tune_choice d = tune_get(p);
+    const mr_geom &g = p->g;
+    const bool has_z = p->cfg.n_spatial == 3;
+    const bool fixed_ok = mr_env_int("MR_AHA_B200_NO_FIXED", 0) == 0;
+    // pass 3 coil grouping
+    if (!p->fused) {
+        if (c.nch != d.nch || c.nc3 != d.nc3 || c.nc2 != d.nc2) return false;
+    } else {
+        const int nch0 = fixed_ok ? mr_fixed_xbdh_coils(g.m[0], g.n[0], g.L) : 0;
+        const int nc2_0 = p->ax[0].small && mr_env_int("MR_AHA_B200_FFT_V1", 0) == 0
+                              ? mr_xbd2_coils(g.m[0], g.L, p->cfg.n_coils, (size_t)mr_smem_limit())
+                              : 0;
+        int ncs[8];
+        const int nn = fixed_ok ? mr_fixed_xbd_list(g.m[0], g.L, ncs, 8) : 0;
+        if (c.nch != d.nch && c.nch != 0 && c.nch != nch0) return false;
+        if (c.nc3 != d.nc3 && c.nc3 != 0 && !tune_in(c.nc3, ncs, nn)) return false;
+        if (c.nc2 != d.nc2 && c.nc2 != 0 && c.nc2 != nc2_0) return false;
+        const bool d_v1 = d.nch == 0 && d.nc3 == 0 && d.nc2 == 0;
+        if (c.nch == 0 && c.nc3 == 0 && c.nc2 == 0 && !d_v1 && !p->v1_fused) return false;
+    }
+    // half-length y passes
+    if (has_z && g.m[1] == 2 * g.n[1] && mr_half_strided_xt(g.n[1], 0) > 0) {
+        int ws[16];
+        const int nw = mr_half_strided_list(g.n[1], ws, 16);
+        if ((c.yh_f == 0) != (c.yh_i == 0)) return false;
+        if (c.yh_f != d.yh_f && c.yh_f != 0 && !tune_in(c.yh_f, ws, nw)) return false;
+        if (c.yh_i != d.yh_i && c.yh_i != 0 && !tune_in(c.yh_i, ws, nw)) return false;
+    } else if (c.yh_f != d.yh_f || c.yh_i != d.yh_i) {
+        return false;
+    }
+    // strided passes: a fixed width, or the generic kernel up to two steps
+    // narrower than the default
+    mr_tune_knob knobs[5];
+    tune_knobs(p, knobs);
+    for (const mr_tune_knob &k : knobs) {
+        const int x3 = c.*k.xt3, xs = c.*k.xts, dx3 = d.*k.xt3, dxs = d.*k.xts;
+        if (!k.on) {
+            if (x3 != dx3 || xs != dxs) return false;
+            continue;
+        }
+        int xts[16];
+        const int nf = fixed_ok ? mr_fixed_strided_list(k.M, k.smode, xts, 16) : 0;
+        if (x3 != dx3 && x3 != 0 && !tune_in(x3, xts, nf)) return false;
+        if (xs != dxs && !(xs >= 0 && xs < dxs && xs >= dxs - 2)) return false;
+    }
+    return true;
+}
+
 static std::mutex g_tune_mu;
 static std::map<std::string, mr_tune_choice> g_tuned;
 
-// Tuned choices of an earlier plan of the same geometry, if any.
+// On-disk cache of tuned choices, shared by processes: the file named by
+// MR_AHA_B200_TUNE_CACHE (none when unset), one line per geometry,
+// "<device name>|<geometry key>|<the choices>". Lines of other devices or
+// that do not parse are ignored; it is read once per process (under
+// g_tune_mu) and rewritten whole (temporary file, then rename) after each
+// autotune.
+static const int kTuneFields = (int)(sizeof(mr_tune_choice) / sizeof(int));
+static bool g_tune_loaded = false;
+
+static std::string tune_device() {
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return "unknown";
+    }
+    return prop.name;
+}
+
+static void tune_load_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char *path = std::getenv("MR_AHA_B200_TUNE_CACHE");
+    if (!path || !path[0]) return;
+    FILE *f = std::fopen(path, "r");
+    if (!f) return;
+    const std::string dev = tune_device();
+    char line[1024];
+    while (std::fgets(line, sizeof(line), f)) {
+        std::string l(line);
+        const size_t a = l.find('|'), b = l.find('|', a == std::string::npos ? a : a + 1);
+        if (a == std::string::npos || b == std::string::npos || l.substr(0, a) != dev) continue;
+        mr_tune_choice c;
+        int *v = reinterpret_cast<int *>(&c);
+        const char *q = l.c_str() + b + 1;
+        int n = 0;
+        for (; n < kTuneFields; ++n) {
+            char *end = nullptr;
+            const long x = std::strtol(q, &end, 10);
+            if (end == q) break;
+            v[n] = (int)x;
+            q = end;
+        }
+        if (n == kTuneFields) g_tuned[l.substr(a + 1, b - a - 1)] = c;
+    }
+    std::fclose(f);
+}
+
+static void tune_save_locked() {
+    const char *path = std::getenv("MR_AHA_B200_TUNE_CACHE");
+    if (!path || !path[0]) return;
+    const std::string dev = tune_device();
+    // keep other devices' lines, replace this device's with the current map
+    std::vector<std::string> keep;
+    if (FILE *f = std::fopen(path, "r")) {
+        char line[1024];
+        while (std::fgets(line, sizeof(line), f)) {
+            std::string l(line);
+            const size_t a = l.find('|');
+            if (a != std::string::npos && l.substr(0, a) != dev) keep.push_back(l);
+        }
+        std::fclose(f);
+    }
+    const std::string tmp = std::string(path) + ".tmp";
+    FILE *f = std::fopen(tmp.c_str(), "w");
+    if (!f) return;
+    for (const std::string &l : keep) std::fputs(l.c_str(), f);
+    for (const auto &kv : g_tuned) {
+        std::fprintf(f, "%s|%s|", dev.c_str(), kv.first.c_str());
+        const int *v = reinterpret_cast<const int *>(&kv.second);
+        for (int n = 0; n < kTuneFields; ++n) std::fprintf(f, " %d", v[n]);
+        std::fputc('\n', f);
+    }
+    const bool ok = std::fclose(f) == 0;
+    if (ok) std::rename(tmp.c_str(), path);
+    else std::remove(tmp.c_str());
+}
+
+// Tuned choices of an earlier plan of the same geometry (this process, or
+// the on-disk cache), if any.
 static void plan_apply_tuned(mr_aha_plan p) {
     std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_load_locked();
     auto it = g_tuned.find(tune_key(p));
-    if (it != g_tuned.end()) tune_set(p, it->second);
+    if (it != g_tuned.end() && tune_valid(p, it->second)) tune_set(p, it->second);
 }
 
 static int tune_time(mr_aha_plan p, const float2 *x, const float2 *S, const mr_kernel_ref &K,
@@ -956,20 +1150,8 @@ int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_k
         }
         tune_set(p, best);
     };
-    // strided passes: (xt3, xts) fields, axis length, store mode, active
-    struct knob {
-        int mr_tune_choice::*xt3;
-        int mr_tune_choice::*xts;
-        int M, smode;
-        bool on;
-    };
-    const knob knobs[] = {
-        {&mr_tune_choice::xt3_z_buf, &mr_tune_choice::xts_z_buf, g.m[2], MR_SM_BUF, has_z},
-        {&mr_tune_choice::xt3_y_buf, &mr_tune_choice::xts_y_buf, g.m[1], MR_SM_BUF, true},
-        {&mr_tune_choice::xt3_yi, &mr_tune_choice::xts_yi, g.m[1], MR_SM_BUF, has_z},
-        {&mr_tune_choice::xt3_y_cs, &mr_tune_choice::xts_y_cs, g.m[1], MR_SM_COILSUM, !has_z},
-        {&mr_tune_choice::xt3_z_cs, &mr_tune_choice::xts_z_cs, g.m[2], MR_SM_COILSUM, has_z},
-    };
+    mr_tune_knob knobs[5];
+    tune_knobs(p, knobs);
     const bool fixed_ok = mr_env_int("MR_AHA_B200_NO_FIXED", 0) == 0;
     // pass 3 first (the largest share), then the strided passes
     if (p->fused && rc == MR_SUCCESS) {
@@ -1031,7 +1213,7 @@ int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_k
                 if (std::memcmp(&c, &base, sizeof(c)) != 0) trial(c);
         }
     }
-    for (const knob &k : knobs) {
+    for (const mr_tune_knob &k : knobs) {
         if (!k.on || rc != MR_SUCCESS) continue;
         const mr_tune_choice base = best;
         std::vector<mr_tune_choice> cands;
@@ -1058,7 +1240,9 @@ int mr_plan_autotune(mr_aha_plan p, const float2 *x, const float2 *S, const mr_k
     tune_set(p, best);
     {
         std::lock_guard<std::mutex> lk(g_tune_mu);
+        tune_load_locked();
         g_tuned[tune_key(p)] = best;
+        tune_save_locked();
     }
     if (best_ms) *best_ms = best_t;
     if (p->cfg.verbose)
