@@ -13,8 +13,9 @@ Arms:
 * default: the CUDA library. ``value`` = applies/s with inputs resident on
   the GPU (CUDA events on the operator's stream, K timed steps between a
   barrier + synchronize on both sides, max over ranks); ``e2e`` = the same
-  metric through ``op(x)`` with host buffers, the host->device copy of x and
-  the device->host copy of A^H A x inside every step.
+  metric through ``op.apply_host`` (``mr_b200_op_execute_host``) with
+  page-locked host buffers: every step copies x in and A^H A x out, the
+  copies of consecutive steps overlapping the applies around them.
 * ``--impl reference``: the reference has no CPU implementation of the path
   here (its CPU route, FINUFFT, is absent), so this times the FP32 CPU port of
   the reference's apply (``oracle/cpu_port.py``) on all host cores; one step
@@ -56,6 +57,8 @@ def parse():
                     choices=["complex64", "bf16", "int16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-samples", type=int, default=2)
+    ap.add_argument("--cg-size", default="stack320",
+                    help="cg320: the operator's workload (stack320, or slab320 for profiling)")
     ap.add_argument("--tune", action="store_true",
                     help="autotune the kernels of each geometry before timing")
     ap.add_argument("--requests", type=int, default=12, help="serve: number of requests")
@@ -297,26 +300,31 @@ def run_ours(args):
     ms = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     value = replica_throughput(args.steps, world, ms)
 
-    # ---- end-to-end through op(x) with host buffers ----
+    # ---- end-to-end from page-locked host buffers through op.apply_host ----
+    # (mr_b200_op_execute_host): every step copies its input in and its
+    # result out; the copies of consecutive steps overlap the applies around
+    # them. Timed from an event recorded before the first call to one
+    # recorded after the final host_sync (all results in host memory).
     y_h = torch.empty(x_h.shape, dtype=x_h.dtype).pin_memory()
-    xe = torch.empty_like(x)
     for _ in range(2):
-        xe.copy_(x_h, non_blocking=True)
-        op(xe, out=out)
-        y_h.copy_(out, non_blocking=True)
+        op.apply_host(x_h, y_h)
+    op.host_sync()
     if dist:
         dist.barrier()
     torch.cuda.synchronize(dev)
     e0.record(stream)
     for _ in range(args.steps):
-        xe.copy_(x_h, non_blocking=True)
-        op(xe, out=out)
-        y_h.copy_(out, non_blocking=True)
+        op.apply_host(x_h, y_h)
+    op.host_sync()
     e1.record(stream)
     torch.cuda.synchronize(dev)
     ms_e = max_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e_same = bool(torch.equal(y_h, out.cpu()))
+    op.host_release()
     e2e = {"value": replica_throughput(args.steps, world, ms_e), "unit": UNIT,
-           "h2d_bytes_per_step": int(x_h.numel() * 8), "d2h_bytes_per_step": int(y_h.numel() * 8)}
+           "h2d_bytes_per_step": int(x_h.numel() * 8), "d2h_bytes_per_step": int(y_h.numel() * 8),
+           "api": "AhAOp.apply_host (mr_b200_op_execute_host), pinned host buffers, "
+                  "copies pipelined with the applies", "equals_device_apply": e2e_same}
 
     # ---- roofline of the dominant kernel ----
     kb = {"complex64": 8, "bf16": 4, "int16": 4}[args.kernel_format]
@@ -404,7 +412,7 @@ def run_cg(args):
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
-    wl = synth.workload("stack320")
+    wl = synth.workload(args.cg_size)
     x = torch.from_numpy(wl["x"]).to(dev)
     S = torch.from_numpy(wl["SEs"]).to(dev)
     cfg = mr.make_config(wl["traj_type"], wl["n_dim"], wl["L"], phi2_dim=wl["phi2_dim"],
@@ -440,11 +448,11 @@ def run_cg(args):
                     "iterate_rel_l2_vs_complex64": _rel(xs, x_c64),
                     "rr_first_last": [float(rr[0]), float(rr[-1])]}
     op.close()
-    line = {"metric": "CG solves/s (30 iterations, stack320)",
+    line = {"metric": f"CG solves/s (30 iterations, {args.cg_size})",
             "value": res["int16"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
             "higher_is_better": True, "data": "synthetic",
             "dtype": "c64 vectors, FP64 reductions, int16+scale kernel",
-            "config": {"workload": "stack320 CG", "n_iter": n_iter, "noise": 1e-3,
+            "config": {"workload": f"{args.cg_size} CG", "n_iter": n_iter, "noise": 1e-3,
                        "reps": reps},
             "formats": res}
     print(json.dumps(line), flush=True)

@@ -60,6 +60,25 @@ MR_EXPORT int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes);
 #define MR_B200_DEV_ERR_TMA_TIMEOUT 1
 MR_EXPORT int mr_b200_op_device_status(mr_op op, int *status);
 
+/* mr_op_execute (reference include/mr_aha/mr_aha.h:1026) with HOST buffers:
+ * h_x and h_AhAx hold mr_x_size(cfg) complex values in host memory. The call
+ * is asynchronous and pipelined: it queues a copy of h_x into one of two
+ * device slots (own copy stream), the apply on the operator's stream, and the
+ * copy of the result to h_AhAx (second copy stream), and returns; the copies
+ * of consecutive calls overlap the applies around them. Both buffers must
+ * stay valid and h_x unmodified until mr_b200_op_host_sync returns. Overlap
+ * needs page-locked host memory (cudaHostAlloc / cudaHostRegister); pageable
+ * buffers give the same results with the copies serialised. The slots (4 x
+ * the image size on the device) are allocated by the first call and freed by
+ * mr_b200_op_host_release or mr_op_destroy. Not for concurrent calls on one
+ * operator. */
+MR_EXPORT int mr_b200_op_execute_host(mr_op op, const mr_complex *h_x, mr_complex *h_AhAx);
+/* Waits for every queued host-buffer apply of the operator (their results
+ * are then in the host buffers); returns the first CUDA error. */
+MR_EXPORT int mr_b200_op_host_sync(mr_op op);
+/* Waits, then frees the device slots of the host-buffer applies. */
+MR_EXPORT int mr_b200_op_host_release(mr_op op);
+
 /* No reference counterpart. Number of kernels one mr_op_execute launches. */
 MR_EXPORT int mr_b200_op_launches(mr_op op, int *n);
 

@@ -23,6 +23,7 @@ from .api import (  # noqa: F401
     make_config,
     num_tri,
     phi2_toep_shape,
+    pinned_empty,
 )
 
 __version__ = "1.0.0"

@@ -186,6 +186,9 @@ PROTOTYPES = {
     "mr_b200_op_kernel_format": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_op_launches": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_op_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "mr_b200_op_execute_host": (ctypes.c_int, [_P, _P, _P]),
+    "mr_b200_op_host_sync": (ctypes.c_int, [_P]),
+    "mr_b200_op_host_release": (ctypes.c_int, [_P]),
     "mr_b200_trace_launches": (ctypes.c_int, [ctypes.c_int]),
     "mr_b200_trace_read": (_I64, [ctypes.c_char_p, ctypes.c_size_t]),
     "mr_b200_aha_toeplitz_noalloc": (ctypes.c_int, [ctypes.POINTER(MRConfig), _P, _P, _P, _P,

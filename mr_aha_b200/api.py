@@ -334,6 +334,51 @@ def calc_toep_from_psf(cfg: MRConfig, psf, t0: int, out, mask=None):
     return out
 
 
+def _host_ptr(array, name: str, expected: int) -> int:
+    """Address of a complex64, C-contiguous host array (numpy, or a CPU torch
+    tensor) of ``expected`` elements."""
+    import numpy as np  # noqa: PLC0415
+
+    if _is_torch(array):
+        torch = _torch()
+        if array.is_cuda:
+            raise TypeError(f"{name} must be in host memory, got a tensor on {array.device}")
+        if array.dtype != torch.complex64:
+            raise TypeError(f"{name} must have dtype complex64, got {array.dtype}")
+        if not array.is_contiguous():
+            raise ValueError(f"{name} must be C-contiguous; call .contiguous() first")
+        n, ptr = int(array.numel()), int(array.data_ptr())
+    elif isinstance(array, np.ndarray):
+        if array.dtype != np.complex64:
+            raise TypeError(f"{name} must have dtype complex64, got {array.dtype}")
+        if not array.flags["C_CONTIGUOUS"]:
+            raise ValueError(f"{name} must be C-contiguous")
+        if not array.flags["WRITEABLE"] and name == "out":
+            raise ValueError("out must be writeable")
+        n, ptr = int(array.size), int(array.ctypes.data)
+    else:
+        raise TypeError(f"{name} must be a numpy array or a CPU torch tensor, "
+                        f"got {type(array).__name__}")
+    if n != expected:
+        raise ValueError(f"{name} has {n} elements but {expected} were expected")
+    return ptr
+
+
+def _host_empty_like(x):
+    import numpy as np  # noqa: PLC0415
+
+    if _is_torch(x):
+        return _torch().empty(tuple(x.shape), dtype=x.dtype, pin_memory=x.is_pinned())
+    return np.empty(x.shape, dtype=np.complex64)
+
+
+def pinned_empty(shape):
+    """A page-locked complex64 host array (a numpy view of a pinned CPU torch
+    tensor; the array's base keeps the tensor alive): host buffers that let
+    :meth:`AhAOp.apply_host` overlap its copies with applies."""
+    return _torch().empty(tuple(shape), dtype=_torch().complex64, pin_memory=True).numpy()
+
+
 def _out_like(x, out):
     """``out``, or a new complex64 array shaped like ``x`` on its device."""
     return _empty(_shape(x), "complex64", _device_of(x)) if out is None else out
@@ -490,6 +535,7 @@ class AhAOp:
         self._device = _device_of(SEs)
         # arrays the library may keep using in place (MR_OP_SHARE_PRIMARY)
         self._keep = (SEs, mask, _phi2_toep) if share_primary else ()
+        self._host_pending = []
         check(lib.mr_op_create(ctypes.byref(cfg), ctypes.byref(inputs), ctypes.byref(opt),
                                ctypes.byref(self._handle)), "mr_op_create")
         del dev_array
@@ -578,6 +624,36 @@ class AhAOp:
         check(lib.mr_b200_op_device_status(self._handle, ctypes.byref(st)),
               "mr_b200_op_device_status")
         return int(st.value)
+
+    def apply_host(self, x, out=None):
+        """``A^H A x`` from and to HOST memory (``mr_b200_op_execute_host``):
+        ``x`` and ``out`` are complex64, C-contiguous numpy arrays or CPU
+        torch tensors of the image's size (``out`` is allocated like ``x``
+        when None). Asynchronous and pipelined: the copies of consecutive
+        calls overlap the applies around them when both buffers are
+        page-locked (``pinned_empty``). The result is in ``out`` after
+        :meth:`host_sync`; until then neither buffer may change."""
+        self._check_open()
+        m = int(lib.mr_x_size(ctypes.byref(self._cfg)))
+        if out is None:
+            out = _host_empty_like(x)
+        px = _host_ptr(x, "x", m)
+        po = _host_ptr(out, "out", m)
+        check(lib.mr_b200_op_execute_host(self._handle, px, po), "mr_b200_op_execute_host")
+        self._host_pending.append((x, out))
+        return out
+
+    def host_sync(self) -> None:
+        """Wait for every queued :meth:`apply_host` (``mr_b200_op_host_sync``)."""
+        self._check_open()
+        check(lib.mr_b200_op_host_sync(self._handle), "mr_b200_op_host_sync")
+        self._host_pending.clear()
+
+    def host_release(self) -> None:
+        """Wait, then free the device slots of :meth:`apply_host`."""
+        self._check_open()
+        check(lib.mr_b200_op_host_release(self._handle), "mr_b200_op_host_release")
+        self._host_pending.clear()
 
     @property
     def launches_per_apply(self) -> int:

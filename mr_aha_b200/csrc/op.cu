@@ -38,7 +38,38 @@ struct mr_op_s {
     float *K16_scale;
     mr_nufft_op *nu;        // MR_OP_NUFFT engine, NULL for the Toeplitz method
     mr_op_info_t info;
+    struct host_pipe *hp;   // host-buffer applies (mr_b200_op_execute_host), NULL until used
 };
+
+// Two device slots (input, output) for applies from and to host memory, a
+// copy stream per direction, and per slot the events that order the three
+// stages of one apply: copy in -> apply on the operator's stream -> copy out.
+// Slot k of call i is reused by call i + 2 once call i's apply has read its
+// input and its copy out has read its output.
+struct host_pipe {
+    float2 *dx[2] = {nullptr, nullptr}, *dy[2] = {nullptr, nullptr};
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t in_done[2] = {}, apply_done[2] = {}, out_done[2] = {};
+    bool used[2] = {false, false};
+    int next = 0;
+};
+
+static void host_pipe_free(host_pipe *hp) {
+    if (!hp) return;
+    if (hp->h2d) cudaStreamSynchronize(hp->h2d);
+    if (hp->d2h) cudaStreamSynchronize(hp->d2h);
+    for (int k = 0; k < 2; ++k) {
+        if (hp->dx[k]) cudaFree(hp->dx[k]);
+        if (hp->dy[k]) cudaFree(hp->dy[k]);
+        if (hp->in_done[k]) cudaEventDestroy(hp->in_done[k]);
+        if (hp->apply_done[k]) cudaEventDestroy(hp->apply_done[k]);
+        if (hp->out_done[k]) cudaEventDestroy(hp->out_done[k]);
+    }
+    if (hp->h2d) cudaStreamDestroy(hp->h2d);
+    if (hp->d2h) cudaStreamDestroy(hp->d2h);
+    cudaGetLastError();
+    delete hp;
+}
 
 static void op_release(mr_op op, int skip_device) {
     if (!skip_device) {
@@ -50,6 +81,7 @@ static void op_release(mr_op op, int skip_device) {
         if (op->K16_scale) cudaFree(op->K16_scale);
         if (op->K_blk) cudaFree(op->K_blk);
         mr_nufft_op_destroy(op->nu);
+        host_pipe_free(op->hp);
         cudaGetLastError();
     }
     delete op;
@@ -381,6 +413,123 @@ extern "C" int mr_op_kernel(mr_op op, int k, const mr_complex **d_phi2_toep) {
                 "storage");
     *d_phi2_toep = reinterpret_cast<const mr_complex *>(op->K);
     return MR_SUCCESS;
+}
+
+// ---- applies from and to host memory ----
+
+// Makes the operator's device current; *prev = the device to restore, or -1.
+static int op_push_device(mr_op op, int *prev) {
+    *prev = -1;
+    int cur = 0;
+    MR_CUDA_TRY(cudaGetDevice(&cur));
+    if (cur != op->dev) {
+        MR_CUDA_TRY(cudaSetDevice(op->dev));
+        *prev = cur;
+    }
+    return MR_SUCCESS;
+}
+
+static int host_pipe_create(mr_op op, size_t bytes, host_pipe **out) {
+    host_pipe *hp = new host_pipe();
+    bool ok = cudaStreamCreateWithFlags(&hp->h2d, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&hp->d2h, cudaStreamNonBlocking) == cudaSuccess;
+    for (int k = 0; k < 2 && ok; ++k)
+        ok = cudaEventCreateWithFlags(&hp->in_done[k], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&hp->apply_done[k], cudaEventDisableTiming) ==
+                 cudaSuccess &&
+             cudaEventCreateWithFlags(&hp->out_done[k], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        host_pipe_free(hp);
+        MR_FAIL(MR_ERR_CUDA, "host-buffer apply: cannot create streams or events");
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (cudaMalloc(&hp->dx[k], bytes) != cudaSuccess ||
+            cudaMalloc(&hp->dy[k], bytes) != cudaSuccess) {
+            host_pipe_free(hp);
+            MR_FAIL(MR_ERR_ALLOC, "host-buffer apply: cannot allocate 4 x %zu bytes", bytes);
+        }
+    }
+    (void)op;
+    *out = hp;
+    return MR_SUCCESS;
+}
+
+static int execute_host_impl(mr_op op, const mr_complex *h_x, mr_complex *h_AhAx) {
+    const size_t bytes = (size_t)mr_x_size(&op->cfg) * sizeof(float2);
+    if (!op->hp) {
+        const int rc = host_pipe_create(op, bytes, &op->hp);
+        if (rc != MR_SUCCESS) return rc;
+    }
+    host_pipe *hp = op->hp;
+    const int k = hp->next;
+    // copy in, once the apply two calls back has read this slot's input
+    if (hp->used[k]) MR_CUDA_TRY(cudaStreamWaitEvent(hp->h2d, hp->apply_done[k], 0));
+    MR_CUDA_TRY(cudaMemcpyAsync(hp->dx[k], h_x, bytes, cudaMemcpyHostToDevice, hp->h2d));
+    MR_CUDA_TRY(cudaEventRecord(hp->in_done[k], hp->h2d));
+    // apply, once the input is in and the copy out two calls back has read
+    // this slot's output
+    MR_CUDA_TRY(cudaStreamWaitEvent(op->stream, hp->in_done[k], 0));
+    if (hp->used[k]) MR_CUDA_TRY(cudaStreamWaitEvent(op->stream, hp->out_done[k], 0));
+    const int rc = mr_op_execute_on(op, hp->dx[k], hp->dy[k], op->stream);
+    if (rc != MR_SUCCESS) return rc;
+    MR_CUDA_TRY(cudaEventRecord(hp->apply_done[k], op->stream));
+    // copy out
+    MR_CUDA_TRY(cudaStreamWaitEvent(hp->d2h, hp->apply_done[k], 0));
+    MR_CUDA_TRY(cudaMemcpyAsync(h_AhAx, hp->dy[k], bytes, cudaMemcpyDeviceToHost, hp->d2h));
+    MR_CUDA_TRY(cudaEventRecord(hp->out_done[k], hp->d2h));
+    hp->used[k] = true;
+    hp->next = k ^ 1;
+    return MR_SUCCESS;
+}
+
+extern "C" int mr_b200_op_execute_host(mr_op op, const mr_complex *h_x, mr_complex *h_AhAx) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_execute_host: op is NULL");
+    MR_REQUIRE(h_x != nullptr, "mr_b200_op_execute_host: h_x is NULL");
+    MR_REQUIRE(h_AhAx != nullptr, "mr_b200_op_execute_host: h_AhAx is NULL");
+    MR_REQUIRE((const void *)h_AhAx != (const void *)h_x,
+               "mr_b200_op_execute_host: h_AhAx must not alias h_x");
+    int prev = -1;
+    int rc = op_push_device(op, &prev);
+    if (rc == MR_SUCCESS) rc = execute_host_impl(op, h_x, h_AhAx);
+    mr_pop_device(prev);
+    return rc;
+}
+
+extern "C" int mr_b200_op_host_sync(mr_op op) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_host_sync: op is NULL");
+    if (!op->hp) return MR_SUCCESS;
+    int prev = -1;
+    int rc = op_push_device(op, &prev);
+    if (rc == MR_SUCCESS) {
+        const cudaError_t e1 = cudaStreamSynchronize(op->hp->h2d);
+        const cudaError_t e2 = cudaStreamSynchronize(op->stream);
+        const cudaError_t e3 = cudaStreamSynchronize(op->hp->d2h);
+        const cudaError_t e = e1 != cudaSuccess ? e1 : (e2 != cudaSuccess ? e2 : e3);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            mr_pop_device(prev);
+            MR_FAIL(MR_ERR_CUDA, "mr_b200_op_host_sync: %s", cudaGetErrorString(e));
+        }
+    }
+    mr_pop_device(prev);
+    return rc;
+}
+
+extern "C" int mr_b200_op_host_release(mr_op op) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr, "mr_b200_op_host_release: op is NULL");
+    if (!op->hp) return MR_SUCCESS;
+    int prev = -1;
+    int rc = op_push_device(op, &prev);
+    if (rc == MR_SUCCESS) {
+        cudaStreamSynchronize(op->stream);
+        host_pipe_free(op->hp);
+        op->hp = nullptr;
+    }
+    mr_pop_device(prev);
+    return rc;
 }
 
 extern "C" int mr_op_destroy(mr_op op) {

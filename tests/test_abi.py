@@ -182,6 +182,31 @@ def test_python_binding_validation():
                         np.zeros((10, 8, 128, 128), np.complex64))
 
 
+def test_host_buffer_validation():
+    """Host-buffer arguments of ``AhAOp.apply_host``: dtype, layout, size and
+    memory kind are checked before any call into the library."""
+    import numpy as np
+    import torch
+
+    from mr_aha_b200.api import _host_ptr, pinned_empty
+
+    a = np.zeros((2, 3), np.complex64)
+    assert _host_ptr(a, "x", 6) == a.ctypes.data
+    t = torch.zeros(6, dtype=torch.complex64)
+    assert _host_ptr(t, "x", 6) == t.data_ptr()
+    with pytest.raises(TypeError):
+        _host_ptr(a.astype(np.complex128), "x", 6)
+    with pytest.raises(ValueError):
+        _host_ptr(np.zeros((3, 4), np.complex64)[:, ::2], "x", 6)
+    with pytest.raises(ValueError):
+        _host_ptr(a, "x", 7)
+    with pytest.raises(TypeError):
+        _host_ptr([0j] * 6, "x", 6)
+    if torch.cuda.is_available():
+        p = pinned_empty((2, 3))
+        assert p.dtype == np.complex64 and p.shape == (2, 3)
+
+
 def test_synthetic_workloads_are_seeded():
     from mr_aha_b200 import synth
 
@@ -219,3 +244,7 @@ def test_added_entry_points_reject_null_arguments():
     assert lib.mr_b200_op_autotune(None, 1, None) == -1
     b = ctypes.c_uint64(0)
     assert lib.mr_b200_op_device_bytes(None, ctypes.byref(b)) == -1
+    assert lib.mr_b200_op_execute_host(None, None, None) == -1
+    assert b"op is NULL" in lib.mr_last_error()
+    assert lib.mr_b200_op_host_sync(None) == -1
+    assert lib.mr_b200_op_host_release(None) == -1
