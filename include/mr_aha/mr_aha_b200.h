@@ -31,6 +31,19 @@ MR_EXPORT int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_comple
 /* No reference counterpart. Current kernel format of the operator. */
 MR_EXPORT int mr_b200_op_kernel_format(mr_op op, int *format);
 
+/* Checkpoint of a 16-bit kernel (the reference saves only the complex64 one,
+ * through mr_op_kernel, include/mr_aha/mr_aha.h:1040-1059). Save: copies the
+ * operator's codes -- nloc x ntri (re, im) pairs of 16-bit codes, 4 bytes
+ * each, layout [ntri][nloc]; nloc = num_masked for a masked operator, else
+ * the grid size -- and its nloc float scales into the caller's device
+ * buffers, and reports the format; MR_ERR_UNSUPPORTED when the kernel is
+ * complex64. Load: copies such codes and scales into the operator, which
+ * from then on applies in that 16-bit format only (its complex64 kernel and
+ * blocked copy are released; mr_op_kernel then fails). Synchronous. */
+MR_EXPORT int mr_b200_op_save_kernel16(mr_op op, int *format, void *d_codes, float *d_scale);
+MR_EXPORT int mr_b200_op_load_kernel16(mr_op op, int format, const void *d_codes,
+                                       const float *d_scale);
+
 /* No reference counterpart. One mr_op_execute with a CUDA event recorded on
  * the operator's stream around every kernel: ms[k] is the time of launch k,
  * names + 32*k its NUL-terminated pass name (names may be NULL). Synchronous.

@@ -187,6 +187,8 @@ PROTOTYPES = {
     "mr_b200_op_launches": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_op_device_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int)]),
     "mr_b200_op_execute_host": (ctypes.c_int, [_P, _P, _P]),
+    "mr_b200_op_save_kernel16": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), _P, _P]),
+    "mr_b200_op_load_kernel16": (ctypes.c_int, [_P, ctypes.c_int, _P, _P]),
     "mr_b200_op_host_sync": (ctypes.c_int, [_P]),
     "mr_b200_op_host_release": (ctypes.c_int, [_P]),
     "mr_b200_trace_launches": (ctypes.c_int, [ctypes.c_int]),

@@ -587,6 +587,51 @@ class AhAOp:
               "mr_b200_op_kernel_format")
         return {v: k for k, v in KERNEL_FORMATS.items()}[f.value]
 
+    def _kernel16_shapes(self):
+        ntri = int(lib.mr_num_tri(int(self._cfg.L)))
+        nloc = int(lib.mr_phi2_toep_size(ctypes.byref(self._cfg))) // ntri
+        return (ntri, nloc, 2), (nloc,)
+
+    def save_kernel16(self):
+        """Checkpoint of the 16-bit kernel (``mr_b200_op_save_kernel16``):
+        ``(fmt, codes, scale)`` with ``codes`` a new ``(ntri, nloc, 2)``
+        tensor (int16, or bfloat16 for ``'bf16'``) of (re, im) codes and
+        ``scale`` ``(nloc,)`` float32; value = scale * code per location."""
+        self._check_open()
+        torch = _torch()
+        cshape, sshape = self._kernel16_shapes()
+        fmt = self.kernel_format
+        if fmt == "complex64":
+            raise MRError(-1, "the operator's kernel is complex64; set a 16-bit format first")
+        codes = torch.empty(cshape, dtype=torch.int16 if fmt == "int16" else torch.bfloat16,
+                            device=self._device)
+        scale = torch.empty(sshape, dtype=torch.float32, device=self._device)
+        f = ctypes.c_int(0)
+        check(lib.mr_b200_op_save_kernel16(self._handle, ctypes.byref(f), codes.data_ptr(),
+                                           scale.data_ptr()), "mr_b200_op_save_kernel16")
+        return fmt, codes, scale
+
+    def load_kernel16(self, fmt: str, codes, scale) -> None:
+        """Restore a 16-bit kernel saved by :meth:`save_kernel16`
+        (``mr_b200_op_load_kernel16``); the operator then applies in ``fmt``
+        only (its complex64 kernel is released)."""
+        self._check_open()
+        if fmt not in ("int16", "bf16"):
+            raise ValueError("fmt must be 'int16' or 'bf16'")
+        torch = _torch()
+        cshape, sshape = self._kernel16_shapes()
+        want = torch.int16 if fmt == "int16" else torch.bfloat16
+        for name, t, shp, dt in (("codes", codes, cshape, want),
+                                 ("scale", scale, sshape, torch.float32)):
+            if not _is_torch(t) or not t.is_cuda or t.dtype != dt or not t.is_contiguous():
+                raise TypeError(f"{name} must be a contiguous CUDA tensor of dtype {dt}")
+            if tuple(t.shape) != shp:
+                raise ValueError(f"{name} has shape {tuple(t.shape)}, expected {shp}")
+        check(lib.mr_b200_op_load_kernel16(self._handle, KERNEL_FORMATS[fmt], codes.data_ptr(),
+                                           scale.data_ptr()), "mr_b200_op_load_kernel16")
+        if len(self._keep) == 3:
+            self._keep = (self._keep[0], self._keep[1], None)
+
     def autotune(self, reps: int = 2) -> float:
         """Pick the fastest kernel of every pass by timing full applies
         (``mr_b200_op_autotune``); returns the tuned apply time in ms."""

@@ -662,6 +662,87 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
     return rc;
 }
 
+// Checkpoint of a 16-bit kernel: its codes ([ntri][nloc] (re, im) pairs of
+// 16-bit codes) and per-location scales, copied out of or into the operator.
+extern "C" int mr_b200_op_save_kernel16(mr_op op, int *format, void *d_codes, float *d_scale) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && format != nullptr && d_codes != nullptr && d_scale != nullptr,
+               "mr_b200_op_save_kernel16: NULL argument");
+    if (op->kf == MR_KF_F32 || !op->K16)
+        MR_FAIL(MR_ERR_UNSUPPORTED,
+                "mr_b200_op_save_kernel16: the operator's kernel is not stored in 16 bits");
+    const int64_t nloc = op->cfg.is_masked ? op->cfg.num_masked : mr_pad_size(&op->cfg);
+    const int64_t ntri = mr_num_tri(op->cfg.L);
+    int prev = -1;
+    int rc = op_push_device(op, &prev);
+    if (rc == MR_SUCCESS) {
+        const cudaError_t e1 = cudaMemcpyAsync(d_codes, op->K16, (size_t)nloc * ntri * 4,
+                                               cudaMemcpyDeviceToDevice, op->stream);
+        const cudaError_t e2 = cudaMemcpyAsync(d_scale, op->K16_scale, (size_t)nloc * sizeof(float),
+                                               cudaMemcpyDeviceToDevice, op->stream);
+        const cudaError_t e3 = cudaStreamSynchronize(op->stream);
+        if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+            cudaGetLastError();
+            rc = MR_ERR_CUDA;
+            mr_set_error("mr_b200_op_save_kernel16: copy failed");
+        } else {
+            *format = op->kf == MR_KF_I16 ? MR_B200_KF_INT16 : MR_B200_KF_BF16;
+        }
+    }
+    mr_pop_device(prev);
+    return rc;
+}
+
+extern "C" int mr_b200_op_load_kernel16(mr_op op, int format, const void *d_codes,
+                                        const float *d_scale) {
+    mr_clear_error();
+    MR_REQUIRE(op != nullptr && d_codes != nullptr && d_scale != nullptr,
+               "mr_b200_op_load_kernel16: NULL argument");
+    MR_REQUIRE(format == MR_B200_KF_BF16 || format == MR_B200_KF_INT16,
+               "mr_b200_op_load_kernel16: format %d is not a 16-bit format", format);
+    if (op->nu)
+        MR_FAIL(MR_ERR_UNSUPPORTED, "mr_b200_op_load_kernel16: a NUFFT operator has no kernel");
+    const int64_t nloc = op->cfg.is_masked ? op->cfg.num_masked : mr_pad_size(&op->cfg);
+    const int64_t ntri = mr_num_tri(op->cfg.L);
+    int prev = -1;
+    int rc = op_push_device(op, &prev);
+    if (rc != MR_SUCCESS) return rc;
+    void *codes = op->K16;
+    float *scale = op->K16_scale;
+    if (!codes && cudaMalloc(&codes, (size_t)nloc * ntri * 4) != cudaSuccess) codes = nullptr;
+    if (codes && !scale && cudaMalloc(&scale, (size_t)nloc * sizeof(float)) != cudaSuccess)
+        scale = nullptr;
+    if (!codes || !scale) {
+        cudaGetLastError();
+        if (codes && codes != op->K16) cudaFree(codes);
+        mr_pop_device(prev);
+        MR_FAIL(MR_ERR_ALLOC, "mr_b200_op_load_kernel16: cannot allocate the 16-bit kernel");
+    }
+    op->K16 = codes;
+    op->K16_scale = scale;
+    const cudaError_t e1 = cudaMemcpyAsync(codes, d_codes, (size_t)nloc * ntri * 4,
+                                           cudaMemcpyDeviceToDevice, op->stream);
+    const cudaError_t e2 = cudaMemcpyAsync(scale, d_scale, (size_t)nloc * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, op->stream);
+    const cudaError_t e3 = cudaStreamSynchronize(op->stream);
+    if (e1 != cudaSuccess || e2 != cudaSuccess || e3 != cudaSuccess) {
+        cudaGetLastError();
+        mr_pop_device(prev);
+        MR_FAIL(MR_ERR_CUDA, "mr_b200_op_load_kernel16: copy failed");
+    }
+    // the loaded codes replace the kernel: the complex64 one (and its blocked
+    // copy) no longer describe this operator
+    if (op->K_own) cudaFree(op->K_own);
+    if (op->K_blk) cudaFree(op->K_blk);
+    op->K_own = nullptr;
+    op->K_blk = nullptr;
+    op->K = nullptr;
+    op->kf = format == MR_B200_KF_INT16 ? MR_KF_I16 : MR_KF_BF16;
+    op->info.toep_source = MR_OP_TOEP_SUPPLIED;
+    mr_pop_device(prev);
+    return MR_SUCCESS;
+}
+
 extern "C" int mr_b200_op_kernel_format(mr_op op, int *format) {
     mr_clear_error();
     MR_REQUIRE(op != nullptr && format != nullptr, "mr_b200_op_kernel_format: NULL argument");

@@ -248,3 +248,6 @@ def test_added_entry_points_reject_null_arguments():
     assert b"op is NULL" in lib.mr_last_error()
     assert lib.mr_b200_op_host_sync(None) == -1
     assert lib.mr_b200_op_host_release(None) == -1
+    f = ctypes.c_int(0)
+    assert lib.mr_b200_op_save_kernel16(None, ctypes.byref(f), None, None) == -1
+    assert lib.mr_b200_op_load_kernel16(None, 2, None, None) == -1
