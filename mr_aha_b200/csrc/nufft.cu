@@ -19,11 +19,17 @@
 // beta = 0.97 pi (1 - 1 / (2 sigma)) w.
 //
 // Spreading runs one thread per (plane, sample) pair with atomic adds into
-// global memory, in FP32 or (for the Toeplitz kernel build) FP64; the FFTs
+// global memory, in FP32 or (for the Toeplitz kernel build) FP64, visiting
+// the samples of a plane in grid-bin order (a permutation sorted once per
+// plan) so that neighbouring threads update neighbouring grid points and the
+// atomics find their lines in L2; the FFTs
 // along each axis are the library's strided / row passes, whose load and
 // store windows also do the zero padding (type 2) and the cropping to the
 // centred modes (type 1).
 #include "nufft.h"
+
+#include <thrust/execution_policy.h>
+#include <thrust/sort.h>
 
 #include <algorithm>
 #include <cmath>
@@ -45,6 +51,7 @@ struct mr_nufft {
     float2 *fine;        // maxp grids
     double2 *fine64;     // maxp grids (fp64 spreading)
     float2 *A, *B, *D;   // FFT stage buffers
+    int *perm;           // samples in grid-bin order, NULL for trajectory order
 };
 
 namespace {
@@ -176,14 +183,15 @@ template <int DIMS, typename R>
 __global__ void __launch_bounds__(256) k_spread(typename cplx<R>::T *fine, const void *cv,
                                                 int64_t cstride, int64_t bcast, int n,
                                                 const float *__restrict__ traj, int64_t npts,
-                                                int nfx, int nfy, int nfz, int w, double beta) {
+                                                const int *__restrict__ perm, int nfx, int nfy,
+                                                int nfz, int w, double beta) {
     using C = typename cplx<R>::T;
     const C *c = reinterpret_cast<const C *>(cv);
     const int64_t nfvol = (int64_t)nfx * nfy * nfz;
     const int64_t total = (int64_t)n * npts;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
          q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t m = q % npts;
+        const int64_t m = perm ? (int64_t)__ldg(perm + q % npts) : q % npts;
         const int p = (int)(q / npts);
         const C v = c[p * cstride + (bcast > 0 ? m % bcast : m)];
         if (v.x == 0 && v.y == 0) continue;
@@ -220,12 +228,13 @@ template <int DIMS>
 __global__ void __launch_bounds__(256) k_interp(float2 *c, int64_t cstride, int n,
                                                 const float2 *__restrict__ fine,
                                                 const float *__restrict__ traj, int64_t npts,
-                                                int nfx, int nfy, int nfz, int w, double beta) {
+                                                const int *__restrict__ perm, int nfx, int nfy,
+                                                int nfz, int w, double beta) {
     const int64_t nfvol = (int64_t)nfx * nfy * nfz;
     const int64_t total = (int64_t)n * npts;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total;
          q += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t m = q % npts;
+        const int64_t m = perm ? (int64_t)__ldg(perm + q % npts) : q % npts;
         const int p = (int)(q / npts);
         float wx[16], wy[16], wz[16];
         const int lx0 = es_axis<float>(__ldg(traj + m), nfx, w, beta, wx);
@@ -256,6 +265,26 @@ __global__ void __launch_bounds__(256) k_interp(float2 *c, int64_t cstride, int 
             }
         }
         c[p * cstride + m] = acc;
+    }
+}
+
+// Grid bin of every sample's nearest grid point below it (bins of bs points
+// per axis, nb[d] bins along axis d, x fastest) and the identity
+// permutation, to be sorted by bin.
+__global__ void k_bin_keys(const float *__restrict__ traj, int64_t npts, int dims, int nfx,
+                           int nfy, int nfz, int bs, int nbx, int nby, int *keys, int *perm) {
+    for (int64_t m = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; m < npts;
+         m += (int64_t)gridDim.x * blockDim.x) {
+        const int nf[3] = {nfx, nfy, nfz};
+        int b[3] = {0, 0, 0};
+        for (int d = 0; d < dims; ++d) {
+            const double u = (double)__ldg(traj + d * npts + m) * nf[d] * (1.0 / (2.0 * kPi));
+            int64_t l = (int64_t)floor(u) % nf[d];
+            if (l < 0) l += nf[d];
+            b[d] = (int)(l / bs);
+        }
+        keys[m] = (b[2] * nby + b[1]) * nbx + b[0];
+        perm[m] = (int)m;
     }
 }
 
@@ -365,7 +394,7 @@ void mr_nufft_grid(const mr_nufft *p, int *nf) {
 void mr_nufft_destroy(mr_nufft *p) {
     if (!p) return;
     for (void *q : {(void *)p->tw, (void *)p->ideconv, (void *)p->fine, (void *)p->fine64,
-                    (void *)p->A, (void *)p->B, (void *)p->D})
+                    (void *)p->A, (void *)p->B, (void *)p->D, (void *)p->perm})
         if (q) cudaFree(q);
     cudaGetLastError();
     delete p;
@@ -441,6 +470,35 @@ int mr_nufft_create(int dims, const int *modes, const float *traj, int64_t npts,
         MR_FAIL(MR_ERR_CUDA, "NUFFT: uploading the tables failed: %s", cudaGetErrorString(e));
     }
     for (int d = 0; d < 3; ++d) p->ax[d].tw = p->tw + off[d];
+    // samples in grid-bin order (16^3 bins in 3-D, 32^2 in 2-D)
+    if (npts <= 0x7fffffffLL && mr_env_int("MR_AHA_B200_NUFFT_NOSORT", 0) == 0) {
+        const int bs = dims == 3 ? 16 : 32;
+        const int nbx = (int)mr_cdiv(p->nf[0], bs), nby = (int)mr_cdiv(p->nf[1], bs);
+        int *keys = nullptr;
+        e = cudaDeviceSynchronize();  // the caller's trajectory is complete
+        if (e == cudaSuccess) e = cudaMalloc(&p->perm, (size_t)npts * sizeof(int));
+        if (e == cudaSuccess) e = cudaMalloc(&keys, (size_t)npts * sizeof(int));
+        if (e == cudaSuccess) {
+            k_bin_keys<<<grid_of(npts), 256>>>(traj, npts, dims, p->nf[0], p->nf[1], p->nf[2], bs,
+                                                nbx, nby, keys, p->perm);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) {
+            try {
+                thrust::sort_by_key(thrust::device, keys, keys + npts, p->perm);
+                e = cudaDeviceSynchronize();
+            } catch (...) {
+                e = cudaErrorUnknown;
+            }
+        }
+        if (keys) cudaFree(keys);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            mr_nufft_destroy(p);
+            MR_FAIL(MR_ERR_CUDA, "NUFFT: sorting the samples by grid bin failed: %s",
+                    cudaGetErrorString(e));
+        }
+    }
     *out = p;
     return MR_SUCCESS;
 }
@@ -457,12 +515,12 @@ int mr_nufft_type1(mr_nufft *p, int iflag, const void *c, int64_t cstride, int64
         MR_CUDA_TRY(cudaMemsetAsync(p->fine64, 0, (size_t)n * nfvol * sizeof(double2), s));
         if (p->dims == 3)
             k_spread<3, double><<<grid_of(total), 256, 0, s>>>(p->fine64, c, cstride, bcast, n,
-                                                               p->traj, p->npts, nfx, nfy, nfz,
-                                                               p->w, p->beta);
+                                                               p->traj, p->npts, p->perm, nfx, nfy,
+                                                               nfz, p->w, p->beta);
         else
             k_spread<2, double><<<grid_of(total), 256, 0, s>>>(p->fine64, c, cstride, bcast, n,
-                                                               p->traj, p->npts, nfx, nfy, nfz,
-                                                               p->w, p->beta);
+                                                               p->traj, p->npts, p->perm, nfx, nfy,
+                                                               nfz, p->w, p->beta);
         MR_LAUNCH_CHECK("k_spread");
         k_narrow<<<grid_of(n * nfvol), 256, 0, s>>>(p->fine, p->fine64, n * nfvol);
         MR_LAUNCH_CHECK("k_narrow");
@@ -470,12 +528,12 @@ int mr_nufft_type1(mr_nufft *p, int iflag, const void *c, int64_t cstride, int64
         MR_CUDA_TRY(cudaMemsetAsync(p->fine, 0, (size_t)n * nfvol * sizeof(float2), s));
         if (p->dims == 3)
             k_spread<3, float><<<grid_of(total), 256, 0, s>>>(p->fine, c, cstride, bcast, n,
-                                                              p->traj, p->npts, nfx, nfy, nfz,
-                                                              p->w, p->beta);
+                                                              p->traj, p->npts, p->perm, nfx, nfy,
+                                                              nfz, p->w, p->beta);
         else
             k_spread<2, float><<<grid_of(total), 256, 0, s>>>(p->fine, c, cstride, bcast, n,
-                                                              p->traj, p->npts, nfx, nfy, nfz,
-                                                              p->w, p->beta);
+                                                              p->traj, p->npts, p->perm, nfx, nfy,
+                                                              nfz, p->w, p->beta);
         MR_LAUNCH_CHECK("k_spread");
     }
     // x: grid rows -> the Mx centred modes
@@ -529,11 +587,11 @@ int mr_nufft_type2(mr_nufft *p, int iflag, const float2 *f, int n, float2 *c, in
     if (rc != MR_SUCCESS) return rc;
     const int64_t total = (int64_t)n * p->npts;
     if (p->dims == 3)
-        k_interp<3><<<grid_of(total), 256, 0, s>>>(c, cstride, n, p->fine, p->traj, p->npts, nfx,
-                                                   nfy, nfz, p->w, p->beta);
+        k_interp<3><<<grid_of(total), 256, 0, s>>>(c, cstride, n, p->fine, p->traj, p->npts,
+                                                   p->perm, nfx, nfy, nfz, p->w, p->beta);
     else
-        k_interp<2><<<grid_of(total), 256, 0, s>>>(c, cstride, n, p->fine, p->traj, p->npts, nfx,
-                                                   nfy, nfz, p->w, p->beta);
+        k_interp<2><<<grid_of(total), 256, 0, s>>>(c, cstride, n, p->fine, p->traj, p->npts,
+                                                   p->perm, nfx, nfy, nfz, p->w, p->beta);
     MR_LAUNCH_CHECK("k_interp");
     return MR_SUCCESS;
 }

@@ -288,8 +288,11 @@ static int toep_spread_build(const mr_config *cfg, const double2 *T, const float
 // Which build a configuration takes: MR_AHA_B200_TOEP_METHOD = 1 forces the
 // spreading build, 2 the closed form; otherwise the cheaper by a cost model
 // calibrated on B200 (3-D 64^3 image, 128^3 grid, L = 4, 2000 x 128
-// samples: closed form 0.59 s, about 8 TFLOP/s of FP64 GEMM; spreading
-// 0.04 s, about 9e10 double atomic adds per second, taken as 5e10 here).
+// samples: closed form 0.59 s, about 8 TFLOP/s of FP64 GEMM; spreading in
+// trajectory order 0.04 s, about 9e10 double atomic adds per second; with
+// the samples in grid-bin order the 3-D kooshball build (256^3 grid, 10000 x
+// 256 samples) runs 1.9x and the stack320 one 1.5x faster: 1e11 here, still
+// pessimistic like the GEMM rate, so the ratio of the two decides).
 static bool use_spread_build(const mr_config *cfg, int64_t Ntrajs, int64_t Nkx) {
     const int m = mr_env_int("MR_AHA_B200_TOEP_METHOD", 0);
     if (m == 1) return true;
@@ -304,7 +307,7 @@ static bool use_spread_build(const mr_config *cfg, int64_t Ntrajs, int64_t Nkx) 
     const double w = 9, wd = three ? w * w * w : w * w;
     const double fine = grid * (three ? 8.0 : 4.0);
     const double t_spread =
-        ntri * nkz * (2.0 * smp * wd / 5e10 + 10.0 * fine * std::log2(fine) / 5e12);
+        ntri * nkz * (2.0 * smp * wd / 1e11 + 10.0 * fine * std::log2(fine) / 5e12);
     return t_spread < t_exact;
 }
 
