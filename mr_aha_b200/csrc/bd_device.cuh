@@ -30,8 +30,11 @@ struct mr_kernel_ref {
     const int *inv;       // masked: natural grid index -> mask row, -1 outside; else NULL
     int kf;
     // optional complex64 copy in the blocked layout (unmasked, Mx % 32 == 0):
-    // natural grid order, x in blocks of 32, component t of block b at
-    // blk[(b * ntri + t) * 32 + x % 32]; NULL if absent
+    // natural grid order, x in blocks of 32. Rank <= 16: components in pairs,
+    // with ntri2 = ceil(ntri / 2) component t of block b at
+    // blk[((b * ntri2 + t / 2) * 32 + x % 32) * 2 + t % 2] (an odd ntri pads
+    // its last pair with zeros); rank > 16: component t of block b at
+    // blk[(b * ntri + t) * 32 + x % 32]. NULL if absent.
     const float2 *blk;
 };
 
@@ -84,13 +87,30 @@ struct mr_kload {
     }
 };
 
-// Loader of one location's block from the blocked layout: `base` points at
-// component 0 of the location, component t is 32 elements further per t (a
-// constant offset once the loop over t is unrolled).
+// Components per frequency of the blocked layout: the packed triangle,
+// padded to an even count when paired (rank <= 16).
+__host__ __device__ constexpr int mr_blk_tri(int L) {
+    return L <= 16 ? 2 * ((L * (L + 1) / 2 + 1) / 2) : L * (L + 1) / 2;
+}
+
+// Loader of one location's block from the blocked layout, paired (rank <=
+// 16: `base` points at the location's component pair 0, pair p is 32 pairs
+// further per p, and both components of a pair come from one 16-byte load --
+// the rank-16 walk reads them one after the other, so the two reads share
+// it) or single (component t is 32 elements further per t; the rank-32 walk
+// reads half of its elements out of packed order).
+template <bool PAIR>
 struct mr_kload_blk {
     const float2 *base;
     float s;
-    __device__ __forceinline__ float2 get_raw(int t) const { return __ldg(base + t * 32); }
+    __device__ __forceinline__ float2 get_raw(int t) const {
+        if constexpr (PAIR) {
+            const float4 q = __ldg(reinterpret_cast<const float4 *>(base) + (t >> 1) * 32);
+            return (t & 1) ? make_float2(q.z, q.w) : make_float2(q.x, q.y);
+        } else {
+            return __ldg(base + t * 32);
+        }
+    }
 };
 
 // Loader for the block of location `loc` (row in the kernel array).

@@ -98,27 +98,39 @@ static int copy_dev(void **dst, const void *src, size_t bytes, cudaStream_t s) {
 }
 
 // Blocked copy of the complex64 kernel (mr_kernel_ref::blk): natural grid
-// order with x in blocks of 32; element (t, jx, jy, jz) at
-// ((((jz My + jy) Mx/32 + jx/32) ntri + t) 32 + jx % 32), from the centred
-// reference layout K[t Vpad + cent(jx) + Mx (cent(jy) + My cent(jz))].
+// order with x in blocks of 32 (block b = (jz My + jy) Mx/32 + jx/32), from
+// the centred reference layout K[t Vpad + cent(jx) + Mx (cent(jy) + My
+// cent(jz))]. pair (rank <= 16): with ntri2 = ceil(ntri / 2), element t at
+// ((b ntri2 + t/2) 32 + jx % 32) 2 + t % 2, the pad component of an odd ntri
+// zero; otherwise element t at (b ntri + t) 32 + jx % 32.
 __global__ void k_block_kernel(float2 *__restrict__ out, const float2 *__restrict__ K, int Mx,
-                               int My, int Mz, int64_t ntri) {
+                               int My, int Mz, int64_t ntri, int pair) {
     const int64_t vpad = (int64_t)Mx * My * Mz;
-    const int64_t total = vpad * ntri;
+    const int64_t ntri2 = (ntri + 1) / 2;
+    const int64_t total = vpad * (pair ? 2 * ntri2 : ntri);
     const int nbx = Mx / 32;
     for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
          o += (int64_t)gridDim.x * blockDim.x) {
-        const int lane = (int)(o & 31);
-        const int64_t rest = o >> 5;
-        const int64_t t = rest % ntri;
-        const int64_t b = rest / ntri;
+        int lane;
+        int64_t t, b;
+        if (pair) {
+            lane = (int)((o >> 1) & 31);
+            const int64_t rest = o >> 6;
+            t = 2 * (rest % ntri2) + (o & 1);
+            b = rest / ntri2;
+        } else {
+            lane = (int)(o & 31);
+            const int64_t rest = o >> 5;
+            t = rest % ntri;
+            b = rest / ntri;
+        }
         const int jx = (int)(b % nbx) * 32 + lane;
         const int64_t yz = b / nbx;
         const int jy = (int)(yz % My), jz = (int)(yz / My);
         const int64_t row = mr_nat2cent_d(jx, Mx, Mx / 2) +
                             (int64_t)Mx * (mr_nat2cent_d(jy, My, My / 2) +
                                            (int64_t)My * mr_nat2cent_d(jz, Mz, Mz / 2));
-        out[o] = K[t * vpad + row];
+        out[o] = t < ntri ? K[t * vpad + row] : make_float2(0.f, 0.f);
     }
 }
 
@@ -133,7 +145,7 @@ static void op_build_blocked(mr_op op) {
     mr_geom g;
     mr_geom_from_config(&op->cfg, &g);
     const int64_t ntri = mr_num_tri(op->cfg.L);
-    const size_t bytes = (size_t)g.vpad * ntri * sizeof(float2);
+    const size_t bytes = (size_t)g.vpad * mr_blk_tri(op->cfg.L) * sizeof(float2);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + ((size_t)2 << 30)) {
         cudaGetLastError();
@@ -145,7 +157,7 @@ static void op_build_blocked(mr_op op) {
         return;
     }
     k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1], g.m[2],
-                                                     ntri);
+                                                     ntri, op->cfg.L <= 16 ? 1 : 0);
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(op->stream) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(op->K_blk);
@@ -859,7 +871,7 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     uint64_t b = op->plan ? mr_plan_device_bytes(op->plan) : 0;
     if (op->K_own) b += nloc * ntri * sizeof(float2);
     if (op->K16) b += nloc * ntri * 4 + nloc * sizeof(float);
-    if (op->K_blk) b += nloc * ntri * sizeof(float2);
+    if (op->K_blk) b += nloc * (uint64_t)mr_blk_tri(c->L) * sizeof(float2);
     if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
     if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
     b += mr_nufft_op_bytes(op->nu);

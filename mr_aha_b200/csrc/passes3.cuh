@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
         // of a location start together and would otherwise all wait for the
         // first one's DRAM reads in the block multiply (43.7 against 44.4 ms
         // at 320 x 320 x 56, L = 16, 12 coils)
-        constexpr int64_t LOCB = (int64_t)((N + 15) / 16) * (L * (L + 1) / 2) * 32 * 8;
+        constexpr int64_t LOCB = (int64_t)((N + 15) / 16) * mr_blk_tri(L) * 32 * 8;
         const int64_t per = ((LOCB / a.nchunk) + 4095) / 4096 * 4096;
         const int64_t b0 = (int64_t)chunk * per, b1 = min(LOCB, b0 + per);
         const char *kb = reinterpret_cast<const char *>(a.K.blk) + (int64_t)loc * LOCB;
@@ -339,10 +339,11 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[i] = make_float2(0.f, 0.f);
                 } else if constexpr (BLK) {
-                    constexpr int NTRI = L * (L + 1) / 2;
-                    const mr_kload_blk kl{a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
-                                                        (NTRI * 32) + (2 * (lane & 15) + par),
-                                          1.f};
+                    const mr_kload_blk<false> kl{
+                        a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
+                                      (mr_blk_tri(L) * 32) +
+                            (2 * (lane & 15) + par),
+                        1.f};
                     if (a.upper) {
                         if (h) bd_half32<1, true, KF>(line, 2 * LS, kl, y);
                         else bd_half32<0, true, KF>(line, 2 * LS, kl, y);
@@ -394,10 +395,11 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
 #pragma unroll
             for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
         } else if constexpr (BLK) {
-            constexpr int NTRI = L * (L + 1) / 2;
-            const mr_kload_blk kl{a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
-                                                (NTRI * 32) + (2 * (lane & 15) + par),
-                                  1.f};
+            // rank <= 16: paired components, two per 16-byte load
+            const mr_kload_blk<true> kl{
+                a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) * (mr_blk_tri(L) * 32) +
+                    2 * (2 * (lane & 15) + par),
+                1.f};
             bd_block<L, 1, KF>(v, y, kl, a.upper);
         } else {
             const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
