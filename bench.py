@@ -673,12 +673,90 @@ def run_toep(args):
     return 0
 
 
+def run_forms(args):
+    """The operator's other forms timed beside the plain Toeplitz apply of the
+    same inputs (CUDA events, after 3 warm-up applies): the masked Toeplitz
+    operator (kernel kept only at the grid locations near samples,
+    mr_calc_mask) at stack320, and the NUFFT-method operator (per coil a
+    type-2 NUFFT, the Gram multiply per sample and a type-1 NUFFT; no kernel)
+    at stack64 and on a 3-D 64^3 kooshball; each with its relative L2 against
+    the plain operator (the masked form drops the kernel outside the mask, so
+    that figure is its approximation error, not rounding)."""
+    import torch
+
+    import mr_aha_b200 as mr
+    from mr_aha_b200 import synth
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    steps = max(3, args.steps // 3)
+
+    def timed(op, x, out):
+        for _ in range(3):
+            op(x, out=out)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            op(x, out=out)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    cases = {
+        "stack320": (synth.workload("stack320"), "masked"),
+        "stack64": (synth.workload("stack64"), "nufft"),
+        "kooshball64": (synth.spec_inputs(dict(traj_type="3D", n_dim=(64, 64, 64), L=4,
+                                               n_coils=4, n_traj=2000, n_kx=128, n_frames=40,
+                                               frame_rule="div", seed=31)), "nufft"),
+    }
+    res = {}
+    for name, (w, form) in cases.items():
+        kw = dict(phi2_dim=w["phi2_dim"], n_coils=w["n_coils"], mem_fraction=0.6)
+        cfg = mr.make_config(w["traj_type"], w["n_dim"], w["L"], **kw)
+        x = torch.from_numpy(w["x"]).to(dev)
+        S = torch.from_numpy(w["SEs"]).to(dev)
+        phi2 = torch.from_numpy(w["phi2"]).to(dev)
+        traj = torch.from_numpy(w["traj"]).to(dev)
+        out = torch.empty_like(x)
+        r = {}
+        with mr.create_op(cfg, S, phi2, traj) as op:
+            r["toeplitz_ms"] = timed(op, x, out)
+        y_plain = out.clone()
+        if form == "masked":
+            mask = mr.calc_mask(cfg, traj)
+            mcfg = mr.make_config(w["traj_type"], w["n_dim"], w["L"], is_masked=True,
+                                  num_masked=int(mask.numel()), **kw)
+            with mr.create_op(mcfg, S, phi2, traj, mask=mask) as mop:
+                r["masked_ms"] = timed(mop, x, out)
+            r["num_masked"] = int(mask.numel())
+            r["grid_locations"] = int(np.prod(w["phi2_dim"]))
+            r["masked_vs_unmasked_rel_l2"] = _rel(out, y_plain)
+        else:
+            with mr.create_op(cfg, S, phi2, traj, method="nufft") as nop:
+                r["nufft_ms"] = timed(nop, x, out)
+            r["nufft_vs_toeplitz_rel_l2"] = _rel(out, y_plain)
+        res[name] = r
+        del x, S, phi2, traj, out, y_plain
+        torch.cuda.empty_cache()
+    line = {"metric": "masked Toeplitz A^H A applies/s (stack320)",
+            "value": 1e3 / res["stack320"]["masked_ms"], "unit": "applies/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic", "dtype": "c64",
+            "config": {"workload": "forms", "cases": list(cases), "steps": steps},
+            "forms": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
-        if args.workload in ("cg320", "batch48", "serve", "toep"):
+        if args.workload in ("cg320", "batch48", "serve", "toep", "forms"):
             print(json.dumps({"impl": "reference", "unavailable":
-                              "the reference has no solver, batch or serving loop"}))
+                              "no reference CPU implementation of this workload here: the "
+                              "reference has no solver, batch or serving loop, and its kernel "
+                              "build and NUFFT method run on FINUFFT / cufinufft, absent"}))
             return 0
         return run_reference(args)
     if args.workload == "cg320":
@@ -687,6 +765,8 @@ def main():
         return run_batch(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "forms":
+        return run_forms(args)
     if args.workload == "toep":
         return run_toep(args)
     return run_ours(args)
