@@ -177,6 +177,7 @@ __global__ void k_mask_inverse(int *inv, const int64_t *__restrict__ mask, int64
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= nm) return;
     int64_t c = mask[i];
+    if (c < 0 || c >= g.vpad) return;  // not a grid location
     const int kx = (int)(c % g.m[0]);
     c /= g.m[0];
     const int ky = (int)(c % g.m[1]);
@@ -222,7 +223,7 @@ static size_t plan_bytes(const mr_aha_plan p, int group) {
 }
 
 int mr_plan_half_pass3(mr_aha_plan p) {
-    return p->fused && p->nch > 0 && !p->cfg.is_masked && p->g.m[0] % 32 == 0;
+    return p->fused && p->nch > 0 && p->g.m[0] % 32 == 0;
 }
 
 size_t mr_plan_device_bytes(mr_aha_plan p) {
@@ -471,7 +472,8 @@ int mr_plan_execute_k(mr_aha_plan p, const float2 *x, const float2 *S,
         MR_LAUNCH_CHECK("k_mask_inverse");
         K.inv = p->d_inv;
         K.stride = nm;
-        K.blk = nullptr;
+        // a blocked copy of a masked kernel is in grid order (zero outside
+        // the mask); pass 3 still skips the locations outside the mask
         prof_mark(prof, nv, "mask_inverse", s);
     } else {
         K.inv = nullptr;

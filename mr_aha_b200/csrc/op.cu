@@ -134,6 +134,37 @@ __global__ void k_block_kernel(float2 *__restrict__ out, const float2 *__restric
     }
 }
 
+// Blocked copy of a masked kernel ([ntri][num_masked], row r at the centred
+// grid index mask[r]): every row scattered to its grid location in the layout
+// of k_block_kernel; locations outside the mask keep the zeros of the
+// preceding memset.
+__global__ void k_block_kernel_masked(float2 *__restrict__ out, const float2 *__restrict__ K,
+                                      const int64_t *__restrict__ mask, int64_t nm, int Mx,
+                                      int My, int Mz, int64_t ntri, int pair) {
+    const int64_t ntri2 = (ntri + 1) / 2;
+    const int64_t total = nm * ntri;
+    const int nbx = Mx / 32;
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+         o += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t r = o % nm;
+        const int64_t t = o / nm;
+        int64_t c = __ldg(mask + r);
+        if (c < 0 || c >= (int64_t)Mx * My * Mz) continue;  // not a grid location
+        const int kx = (int)(c % Mx);
+        c /= Mx;
+        const int ky = (int)(c % My);
+        const int kz = (int)(c / My);
+        // centred -> natural index along each axis (inverse of mr_nat2cent_d)
+        const int jx = mr_nat2cent_d(kx, Mx, Mx - Mx / 2);
+        const int jy = mr_nat2cent_d(ky, My, My - My / 2);
+        const int jz = mr_nat2cent_d(kz, Mz, Mz - Mz / 2);
+        const int64_t b = ((int64_t)jz * My + jy) * nbx + jx / 32;
+        const int64_t pos = pair ? ((b * ntri2 + t / 2) * 32 + jx % 32) * 2 + (t & 1)
+                                 : (b * ntri + t) * 32 + jx % 32;
+        out[pos] = K[o];
+    }
+}
+
 // Build the blocked copy when the operator owns its kernel (a borrowed one
 // may change under it), the plan can use it and the device has room for it
 // (it doubles the complex64 kernel's footprint); otherwise leave it out (the
@@ -156,8 +187,20 @@ static void op_build_blocked(mr_op op) {
         op->K_blk = nullptr;
         return;
     }
-    k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1], g.m[2],
-                                                     ntri, op->cfg.L <= 16 ? 1 : 0);
+    const int pair = op->cfg.L <= 16 ? 1 : 0;
+    if (op->cfg.is_masked) {
+        if (cudaMemsetAsync(op->K_blk, 0, bytes, op->stream) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFree(op->K_blk);
+            op->K_blk = nullptr;
+            return;
+        }
+        k_block_kernel_masked<<<148 * 16, 256, 0, op->stream>>>(
+            op->K_blk, op->K, op->mask, op->cfg.num_masked, g.m[0], g.m[1], g.m[2], ntri, pair);
+    } else {
+        k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1],
+                                                         g.m[2], ntri, pair);
+    }
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(op->stream) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(op->K_blk);
@@ -871,7 +914,7 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     uint64_t b = op->plan ? mr_plan_device_bytes(op->plan) : 0;
     if (op->K_own) b += nloc * ntri * sizeof(float2);
     if (op->K16) b += nloc * ntri * 4 + nloc * sizeof(float);
-    if (op->K_blk) b += nloc * (uint64_t)mr_blk_tri(c->L) * sizeof(float2);
+    if (op->K_blk) b += (uint64_t)mr_pad_size(c) * mr_blk_tri(c->L) * sizeof(float2);
     if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
     if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
     b += mr_nufft_op_bytes(op->nu);

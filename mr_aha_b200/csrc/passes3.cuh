@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbd3(const __grid_constant__
 // four length-N transforms of N-sample lines in place of two length-M
 // transforms of half-empty ones. Row b = (coil, rank) of the tile keeps its
 // even half-spectrum in line 2b and its odd one in line 2b + 1. BLK: read
-// the complex64 kernel from its blocked copy (a.K.blk, unmasked only), where
+// the complex64 kernel from its blocked copy (a.K.blk; a masked kernel's copy
+// is in grid order, zero outside the mask, whose locations are still skipped), where
 // the 32 frequencies of a warp are contiguous for every component. TMAIN:
 // the CTA's NC L input rows arrive by TMA tensor copies (a.in_map: extents
 // {N, plane_rows, planes of the group}, box {N or N / 2, 1, NC L}; planes
@@ -1066,7 +1067,7 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
     const int64_t nblk = (int64_t)a.nloc * a.nchunk;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
     if constexpr (KF == MR_KF_F32) {
-        if (a.K.blk && !a.K.inv) {
+        if (a.K.blk) {
             if (mr_env_int("MR_AHA_B200_NO_TMA", 0) == 0 && ((uintptr_t)a.src & 15) == 0 &&
                 (a.s_row & 1) == 0 && a.plane_rows <= 0x7fffffff) {
                 // the group's rows as a 3-D tensor {x, row of a plane, plane}
@@ -1081,14 +1082,15 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
                 static unsigned long long attr_t = 0;
                 set_attr(k_xbdh<N, L, NC, KF, kNT, true, true>, attr_t);
                 k_xbdh<N, L, NC, KF, kNT, true, true><<<(unsigned)nblk, kNT, smem + 16, s>>>(b);
-                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked,tma>", N, L,
-                                  NC, kNT);
+                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked,tma%s>", N, L,
+                                  NC, kNT, a.K.inv ? ",masked" : "");
                 return MR_SUCCESS;
             }
             static unsigned long long attr_b = 0;
             set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
             k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);
-            MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked>", N, L, NC, kNT);
+            MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked%s>", N, L, NC, kNT,
+                              a.K.inv ? ",masked" : "");
             return MR_SUCCESS;
         }
     }
