@@ -34,8 +34,12 @@ struct mr_kernel_ref {
     // with ntri2 = ceil(ntri / 2) component t of block b at
     // blk[((b * ntri2 + t / 2) * 32 + x % 32) * 2 + t % 2] (an odd ntri pads
     // its last pair with zeros); rank > 16: component t of block b at
-    // blk[(b * ntri + t) * 32 + x % 32]. NULL if absent.
+    // blk[(b * ntri + t) * 32 + x % 32]. 16-bit formats (rank <= 16): the
+    // 4-byte codes in groups of four, with ntri4 = ceil(ntri / 4) code t of
+    // block b at word ((b * ntri4 + t / 4) * 32 + x % 32) * 4 + t % 4, and the
+    // locations' scales in natural grid order in sblk. NULL if absent.
     const float2 *blk;
+    const float *sblk;
 };
 
 // An int16 (re, im) pair as two exact floats without conversion
@@ -92,6 +96,27 @@ struct mr_kload {
 __host__ __device__ constexpr int mr_blk_tri(int L) {
     return L <= 16 ? 2 * ((L * (L + 1) / 2 + 1) / 2) : L * (L + 1) / 2;
 }
+
+// Components per frequency of the 16-bit blocked layout: the packed triangle
+// padded to a multiple of four (four 4-byte codes per 16-byte load).
+__host__ __device__ constexpr int mr_blk16_tri(int L) { return 4 * ((L * (L + 1) / 2 + 3) / 4); }
+
+// Loader of one location's 16-bit block from the blocked layout (rank <=
+// 16): `base` points at the location's group 0, group p is 32 groups further
+// per p, and the four codes of a group come from one 16-byte load that the
+// rank-16 walk's consecutive reads share; `s` is the location's scale (the
+// block multiply scales its result once).
+template <int KF>
+struct mr_kload_blk16 {
+    const uint4 *base;
+    float s;
+    __device__ __forceinline__ float2 get_raw(int t) const {
+        const uint4 q = __ldg(base + (t >> 2) * 32);
+        const uint32_t w = (t & 3) == 0 ? q.x : ((t & 3) == 1 ? q.y : ((t & 3) == 2 ? q.z : q.w));
+        if constexpr (KF == MR_KF_BF16) return mr_bf16x2_to_float2(w);
+        else return mr_i16x2_to_float2(w);
+    }
+};
 
 // Loader of one location's block from the blocked layout, paired (rank <=
 // 16: `base` points at the location's component pair 0, pair p is 32 pairs

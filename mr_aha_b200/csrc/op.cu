@@ -32,6 +32,11 @@ struct mr_op_s {
     // complex64 kernel in the blocked layout read by the half-length pass 3
     // (mr_kernel_ref::blk), NULL when not built
     float2 *K_blk;
+    // 16-bit formats: the codes in a blocked layout (four components per
+    // 16-byte word group, rank <= 16) in K_blk, with the locations' scales in
+    // natural grid order here; blk_kf = format of the copy in K_blk, -1 if none
+    float *K_blk_scale;
+    int blk_kf;
     // 16-bit kernel copy (MR_B200_KF_BF16 / MR_B200_KF_I16) and its scales
     int kf;
     void *K16;
@@ -80,6 +85,7 @@ static void op_release(mr_op op, int skip_device) {
         if (op->K16) cudaFree(op->K16);
         if (op->K16_scale) cudaFree(op->K16_scale);
         if (op->K_blk) cudaFree(op->K_blk);
+        if (op->K_blk_scale) cudaFree(op->K_blk_scale);
         mr_nufft_op_destroy(op->nu);
         host_pipe_free(op->hp);
         cudaGetLastError();
@@ -165,47 +171,108 @@ __global__ void k_block_kernel_masked(float2 *__restrict__ out, const float2 *__
     }
 }
 
-// Build the blocked copy when the operator owns its kernel (a borrowed one
-// may change under it), the plan can use it and the device has room for it
-// (it doubles the complex64 kernel's footprint); otherwise leave it out (the
-// apply then reads the reference layout). Never fails the caller.
+// 16-bit blocked copy: with ntri4 = ceil(ntri / 4), the code of element
+// (t, jx, jy, jz) at word ((b ntri4 + t/4) 32 + jx % 32) 4 + t % 4 (block b as
+// in k_block_kernel; pad components zero), and the location's scale at its
+// natural grid index (b 32 + jx % 32), from the reference-layout codes and
+// scales (row = centred grid index).
+__global__ void k_block_kernel16(uint32_t *__restrict__ out, float *__restrict__ sout,
+                                 const uint32_t *__restrict__ K16, const float *__restrict__ scale,
+                                 int Mx, int My, int Mz, int64_t ntri) {
+    const int64_t vpad = (int64_t)Mx * My * Mz;
+    const int64_t ntri4 = (ntri + 3) / 4;
+    const int64_t total = vpad * 4 * ntri4;
+    const int nbx = Mx / 32;
+    for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < total;
+         o += (int64_t)gridDim.x * blockDim.x) {
+        const int lane = (int)((o >> 2) & 31);
+        const int64_t rest = o >> 7;
+        const int64_t t = 4 * (rest % ntri4) + (o & 3);
+        const int64_t b = rest / ntri4;
+        const int jx = (int)(b % nbx) * 32 + lane;
+        const int64_t yz = b / nbx;
+        const int jy = (int)(yz % My), jz = (int)(yz / My);
+        const int64_t row = mr_nat2cent_d(jx, Mx, Mx / 2) +
+                            (int64_t)Mx * (mr_nat2cent_d(jy, My, My / 2) +
+                                           (int64_t)My * mr_nat2cent_d(jz, Mz, Mz / 2));
+        out[o] = t < ntri ? K16[t * vpad + row] : 0u;
+        if (t == 0) sout[b * 32 + lane] = scale[row];
+    }
+}
+
+static void op_free_blocked(mr_op op) {
+    if (op->K_blk || op->K_blk_scale) cudaStreamSynchronize(op->stream);
+    if (op->K_blk) cudaFree(op->K_blk);
+    if (op->K_blk_scale) cudaFree(op->K_blk_scale);
+    op->K_blk = nullptr;
+    op->K_blk_scale = nullptr;
+    op->blk_kf = -1;
+    cudaGetLastError();
+}
+
+static size_t op_blocked_bytes(const mr_config *cfg, int kf) {
+    const size_t vpad = (size_t)mr_pad_size(cfg);
+    if (kf == MR_KF_F32) return vpad * mr_blk_tri(cfg->L) * sizeof(float2);
+    return vpad * mr_blk16_tri(cfg->L) * 4 + vpad * sizeof(float);
+}
+
+// Build the blocked copy of the current kernel format when the plan can use
+// it and the device has room (it doubles the kernel's footprint); otherwise
+// leave it out (the apply then reads the reference layout). complex64: only
+// for a kernel the operator owns (a borrowed one may change under it); a
+// masked operator's copy covers the whole grid, zero outside the mask.
+// 16-bit: unmasked, rank <= 16. A copy of another format is freed first.
+// Never fails the caller.
 static void op_build_blocked(mr_op op) {
-    if (op->K_blk || !op->K_own || !op->plan || !mr_plan_half_pass3(op->plan) ||
-        mr_env_int("MR_AHA_B200_NO_BLOCKED", 0))
+    if (op->K_blk && op->blk_kf == op->kf) return;
+    op_free_blocked(op);
+    if (!op->plan || !mr_plan_half_pass3(op->plan) || mr_env_int("MR_AHA_B200_NO_BLOCKED", 0))
         return;
+    const bool f32 = op->kf == MR_KF_F32;
+    if (f32 ? !op->K_own : (!op->K16 || op->cfg.is_masked || op->cfg.L > 16)) return;
     mr_geom g;
     mr_geom_from_config(&op->cfg, &g);
     const int64_t ntri = mr_num_tri(op->cfg.L);
-    const size_t bytes = (size_t)g.vpad * mr_blk_tri(op->cfg.L) * sizeof(float2);
+    const size_t bytes = op_blocked_bytes(&op->cfg, op->kf);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + ((size_t)2 << 30)) {
         cudaGetLastError();
         return;
     }
-    if (cudaMalloc(&op->K_blk, bytes) != cudaSuccess) {
+    const size_t sbytes = f32 ? 0 : (size_t)g.vpad * sizeof(float);
+    if (cudaMalloc(&op->K_blk, bytes - sbytes) != cudaSuccess ||
+        (sbytes && cudaMalloc(&op->K_blk_scale, sbytes) != cudaSuccess)) {
         cudaGetLastError();
-        op->K_blk = nullptr;
+        op_free_blocked(op);
         return;
     }
-    const int pair = op->cfg.L <= 16 ? 1 : 0;
-    if (op->cfg.is_masked) {
-        if (cudaMemsetAsync(op->K_blk, 0, bytes, op->stream) != cudaSuccess) {
-            cudaGetLastError();
-            cudaFree(op->K_blk);
-            op->K_blk = nullptr;
-            return;
-        }
-        k_block_kernel_masked<<<148 * 16, 256, 0, op->stream>>>(
-            op->K_blk, op->K, op->mask, op->cfg.num_masked, g.m[0], g.m[1], g.m[2], ntri, pair);
+    if (!f32) {
+        k_block_kernel16<<<148 * 16, 256, 0, op->stream>>>(
+            reinterpret_cast<uint32_t *>(op->K_blk), op->K_blk_scale,
+            reinterpret_cast<const uint32_t *>(op->K16), op->K16_scale, g.m[0], g.m[1], g.m[2],
+            ntri);
     } else {
-        k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1],
-                                                         g.m[2], ntri, pair);
+        const int pair = op->cfg.L <= 16 ? 1 : 0;
+        if (op->cfg.is_masked) {
+            if (cudaMemsetAsync(op->K_blk, 0, bytes, op->stream) != cudaSuccess) {
+                cudaGetLastError();
+                op_free_blocked(op);
+                return;
+            }
+            k_block_kernel_masked<<<148 * 16, 256, 0, op->stream>>>(
+                op->K_blk, op->K, op->mask, op->cfg.num_masked, g.m[0], g.m[1], g.m[2], ntri,
+                pair);
+        } else {
+            k_block_kernel<<<148 * 16, 256, 0, op->stream>>>(op->K_blk, op->K, g.m[0], g.m[1],
+                                                             g.m[2], ntri, pair);
+        }
     }
     if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(op->stream) != cudaSuccess) {
         cudaGetLastError();
-        cudaFree(op->K_blk);
-        op->K_blk = nullptr;
+        op_free_blocked(op);
+        return;
     }
+    op->blk_kf = op->kf;
 }
 
 static int op_check(const mr_config *cfg, const mr_op_inputs *in, const mr_op_options *o) {
@@ -245,6 +312,7 @@ static int op_create_impl(const mr_config *cfg, const mr_op_inputs *in, const mr
     if (rc != MR_SUCCESS) return rc;
     mr_op op = new (std::nothrow) mr_op_s();
     if (!op) MR_FAIL(MR_ERR_ALLOC, "failed to allocate the operator");
+    op->blk_kf = -1;
     op->cfg = *cfg;
     op->opt = *o;
     op->stream = (cudaStream_t)cfg->stream;
@@ -412,10 +480,13 @@ static mr_kernel_ref op_kernel_ref(mr_op op) {
     std::memset(&K, 0, sizeof(K));
     if (op->kf == MR_KF_F32) {
         K.data = op->K;
-        K.blk = op->K_blk;
     } else {
         K.data = op->K16;
         K.scale = op->K16_scale;
+    }
+    if (op->K_blk && op->blk_kf == op->kf) {
+        K.blk = op->K_blk;
+        K.sblk = op->K_blk_scale;
     }
     K.kf = op->kf;
     return K;
@@ -677,10 +748,9 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
     } else {
         const int64_t nloc = op->cfg.is_masked ? op->cfg.num_masked : mr_pad_size(&op->cfg);
         const int64_t ntri = mr_num_tri(op->cfg.L);
-        // the blocked complex64 copy serves only the complex64 format: give
-        // its memory back before the 16-bit copy is allocated
-        if (op->K_blk) cudaFree(op->K_blk);
-        op->K_blk = nullptr;
+        // a blocked copy serves only its own format: give its memory back
+        // before the 16-bit kernel is allocated
+        op_free_blocked(op);
         if (op->K16) cudaFree(op->K16);
         if (op->K16_scale) cudaFree(op->K16_scale);
         op->K16 = nullptr;
@@ -705,11 +775,10 @@ extern "C" int mr_b200_op_set_kernel_format(mr_op op, int format, int keep_compl
                     // an owned copy is freed; a borrowed kernel is handed
                     // back (the caller may free it)
                     if (op->K_own) cudaFree(op->K_own);
-                    if (op->K_blk) cudaFree(op->K_blk);
                     op->K_own = nullptr;
-                    op->K_blk = nullptr;
                     op->K = nullptr;
                 }
+                op_build_blocked(op);
             }
         }
     }
@@ -787,13 +856,13 @@ extern "C" int mr_b200_op_load_kernel16(mr_op op, int format, const void *d_code
     }
     // the loaded codes replace the kernel: the complex64 one (and its blocked
     // copy) no longer describe this operator
+    op_free_blocked(op);
     if (op->K_own) cudaFree(op->K_own);
-    if (op->K_blk) cudaFree(op->K_blk);
     op->K_own = nullptr;
-    op->K_blk = nullptr;
     op->K = nullptr;
     op->kf = format == MR_B200_KF_INT16 ? MR_KF_I16 : MR_KF_BF16;
     op->info.toep_source = MR_OP_TOEP_SUPPLIED;
+    op_build_blocked(op);
     mr_pop_device(prev);
     return MR_SUCCESS;
 }
@@ -893,15 +962,10 @@ extern "C" int mr_b200_op_blocked_copy(mr_op op, int enable, int *built) {
     int prev = 0;
     MR_CUDA_TRY(cudaGetDevice(&prev));
     if (prev != op->dev) MR_CUDA_TRY(cudaSetDevice(op->dev));
-    if (enable) {
-        if (op->kf == MR_KF_F32) op_build_blocked(op);
-    } else if (op->K_blk) {
-        cudaStreamSynchronize(op->stream);
-        cudaFree(op->K_blk);
-        op->K_blk = nullptr;
-    }
+    if (enable) op_build_blocked(op);
+    else op_free_blocked(op);
     if (prev != op->dev) cudaSetDevice(prev);
-    if (built) *built = op->K_blk != nullptr;
+    if (built) *built = op->K_blk != nullptr && op->blk_kf == op->kf;
     return MR_SUCCESS;
 }
 
@@ -914,7 +978,7 @@ extern "C" int mr_b200_op_device_bytes(mr_op op, uint64_t *bytes) {
     uint64_t b = op->plan ? mr_plan_device_bytes(op->plan) : 0;
     if (op->K_own) b += nloc * ntri * sizeof(float2);
     if (op->K16) b += nloc * ntri * 4 + nloc * sizeof(float);
-    if (op->K_blk) b += (uint64_t)mr_pad_size(c) * mr_blk_tri(c->L) * sizeof(float2);
+    if (op->K_blk) b += op_blocked_bytes(c, op->blk_kf);
     if (op->S_own) b += (uint64_t)mr_se_size(c) * sizeof(float2);
     if (op->mask_own) b += (uint64_t)c->num_masked * sizeof(int64_t);
     b += mr_nufft_op_bytes(op->nu);

@@ -236,7 +236,9 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
         // of a location start together and would otherwise all wait for the
         // first one's DRAM reads in the block multiply (43.7 against 44.4 ms
         // at 320 x 320 x 56, L = 16, 12 coils)
-        constexpr int64_t LOCB = (int64_t)((N + 15) / 16) * mr_blk_tri(L) * 32 * 8;
+        constexpr int64_t LOCB = KF == MR_KF_F32
+                                     ? (int64_t)((N + 15) / 16) * mr_blk_tri(L) * 32 * 8
+                                     : (int64_t)((N + 15) / 16) * mr_blk16_tri(L) * 32 * 4;
         const int64_t per = ((LOCB / a.nchunk) + 4095) / 4096 * 4096;
         const int64_t b0 = (int64_t)chunk * per, b1 = min(LOCB, b0 + per);
         const char *kb = reinterpret_cast<const char *>(a.K.blk) + (int64_t)loc * LOCB;
@@ -340,6 +342,7 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
 #pragma unroll
                     for (int i = 0; i < 16; ++i) y[i] = make_float2(0.f, 0.f);
                 } else if constexpr (BLK) {
+                    static_assert(KF == MR_KF_F32, "16-bit blocked copies are for rank <= 16");
                     const mr_kload_blk<false> kl{
                         a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) *
                                       (mr_blk_tri(L) * 32) +
@@ -396,12 +399,19 @@ __global__ void __launch_bounds__(kNT, 512 / kNT) k_xbdh(const __grid_constant__
 #pragma unroll
             for (int l = 0; l < L; ++l) y[0][l] = make_float2(0.f, 0.f);
         } else if constexpr (BLK) {
-            // rank <= 16: paired components, two per 16-byte load
-            const mr_kload_blk<true> kl{
-                a.K.blk + (((int64_t)jz * a.My + jy) * MB + (wi - k * MB)) * (mr_blk_tri(L) * 32) +
-                    2 * (2 * (lane & 15) + par),
-                1.f};
-            bd_block<L, 1, KF>(v, y, kl, a.upper);
+            const int64_t blk = ((int64_t)jz * a.My + jy) * MB + (wi - k * MB);
+            const int f = 2 * (lane & 15) + par;
+            if constexpr (KF == MR_KF_F32) {
+                // rank <= 16: paired components, two per 16-byte load
+                const mr_kload_blk<true> kl{a.K.blk + blk * (mr_blk_tri(L) * 32) + 2 * f, 1.f};
+                bd_block<L, 1, KF>(v, y, kl, a.upper);
+            } else {
+                // four 16-bit codes per 16-byte load, the location's scale
+                const mr_kload_blk16<KF> kl{
+                    reinterpret_cast<const uint4 *>(a.K.blk) + blk * (mr_blk16_tri(L) / 4 * 32) + f,
+                    __ldg(a.K.sblk + blk * 32 + f)};
+                bd_block<L, 1, KF>(v, y, kl, a.upper);
+            }
         } else {
             const mr_kload<KF> kl = mr_kload_at<KF>(a.K, row);
             bd_block<L, 1, KF>(v, y, kl, a.upper);
@@ -1066,7 +1076,10 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
     const size_t smem = (size_t)2 * NC * L * odd_stride<N>() * sizeof(float2);
     const int64_t nblk = (int64_t)a.nloc * a.nchunk;
     if (nblk > 0x7fffffffLL) MR_FAIL(MR_ERR_UNSUPPORTED, "block-diagonal pass grid too large");
-    if constexpr (KF == MR_KF_F32) {
+    constexpr const char *kfs = KF == MR_KF_F32 ? "F32" : (KF == MR_KF_BF16 ? "BF16" : "I16");
+    // blocked kernel copies: complex64 (any rank), 16-bit (rank <= 16, TMA
+    // tiles only; without them the 16-bit pass reads the reference layout)
+    if constexpr (KF == MR_KF_F32 || L <= 16) {
         if (a.K.blk) {
             if (mr_env_int("MR_AHA_B200_NO_TMA", 0) == 0 && ((uintptr_t)a.src & 15) == 0 &&
                 (a.s_row & 1) == 0 && a.plane_rows <= 0x7fffffff) {
@@ -1082,23 +1095,24 @@ int launch_xh(const mr_x_args &a, cudaStream_t s) {
                 static unsigned long long attr_t = 0;
                 set_attr(k_xbdh<N, L, NC, KF, kNT, true, true>, attr_t);
                 k_xbdh<N, L, NC, KF, kNT, true, true><<<(unsigned)nblk, kNT, smem + 16, s>>>(b);
-                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked,tma%s>", N, L,
-                                  NC, kNT, a.K.inv ? ",masked" : "");
+                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,%s,%d,blocked,tma%s>", N, L,
+                                  NC, kfs, kNT, a.K.inv ? ",masked" : "");
                 return MR_SUCCESS;
             }
-            static unsigned long long attr_b = 0;
-            set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
-            k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);
-            MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked%s>", N, L, NC, kNT,
-                              a.K.inv ? ",masked" : "");
-            return MR_SUCCESS;
+            if constexpr (KF == MR_KF_F32) {
+                static unsigned long long attr_b = 0;
+                set_attr(k_xbdh<N, L, NC, KF, kNT, true>, attr_b);
+                k_xbdh<N, L, NC, KF, kNT, true><<<(unsigned)nblk, kNT, smem, s>>>(a);
+                MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,F32,%d,blocked%s>", N, L, NC,
+                                  kNT, a.K.inv ? ",masked" : "");
+                return MR_SUCCESS;
+            }
         }
     }
     static unsigned long long attr = 0;
     set_attr(k_xbdh<N, L, NC, KF, kNT>, attr);
     k_xbdh<N, L, NC, KF, kNT><<<(unsigned)nblk, kNT, smem, s>>>(a);
-    MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,%s,%d%s>", N, L, NC,
-                      KF == MR_KF_F32 ? "F32" : (KF == MR_KF_BF16 ? "BF16" : "I16"), kNT,
+    MR_LAUNCH_CHECK_T("k_xbdh", "k_xbdh<N=%d,L=%d,NC=%d,%s,%d%s>", N, L, NC, kfs, kNT,
                       a.K.inv ? ",masked" : "");
     return MR_SUCCESS;
 }

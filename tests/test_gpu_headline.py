@@ -26,8 +26,9 @@ Checks, relative L2 (tolerances written in each test):
 2. ``slab320``: a 320 x 320 x 4 stack with L = 16 and 3 coils (the headline
    y and x kernels, blocked copy) against the FP64 oracle, <= 1e-5; the same
    with the copy released (reference layout); the int16 and bf16 kernel
-   formats against the FP64 oracle of the values they store (<= 1e-5) and of
-   the complex64 kernel (int16 <= 1e-4, bf16 <= 5e-3).
+   formats (their own blocked copies, bit-identical to the reference layout)
+   against the FP64 oracle of the values they store (<= 1e-5) and of the
+   complex64 kernel (int16 <= 1e-4, bf16 <= 5e-3).
 3. ``stack320``: the full headline workload against the reference's own CUDA
    apply (compiled from its sources into ``oracle/_ref`` by
    ``oracle/Makefile``) given the same kernel, <= 1e-5 (both FP32); with the
@@ -145,13 +146,20 @@ def test_slab320_blocked_and_reference_layout_vs_fp64(slab, monkeypatch):
 @pytest.mark.parametrize("fmt,tol_exact", [("int16", 1e-4), ("bf16", 5e-3)])
 def test_slab320_16bit_vs_fp64(slab, fmt, tol_exact):
     p, op, K, ref = slab
+    kf = "I16" if fmt == "int16" else "BF16"
     op.set_kernel_format(fmt)
     try:
+        # the 16-bit blocked copy (four codes per 16-byte load), then the
+        # reference layout: same codes, same arithmetic, bit-identical
         y, trace = traced(lambda: host(op(dev(p["x"]))))
+        assert f"k_xbdh<N=320,L=16,NC=1,{kf},256,blocked,tma>" in trace, trace
+        assert op.blocked_copy(False) is False
+        y1, trace1 = traced(lambda: host(op(dev(p["x"]))))
+        assert f"k_xbdh<N=320,L=16,NC=1,{kf},256>" in trace1, trace1
+        np.testing.assert_array_equal(y1, y)
     finally:
         op.set_kernel_format("complex64")
-    kf = "I16" if fmt == "int16" else "BF16"
-    assert f"k_xbdh<N=320,L=16,NC=1,{kf},256>" in trace, trace
+    assert op.blocked_copy(True) is True
     same = O.rel_l2(y, _oracle(p, O.dequantized_kernel(K, fmt)))
     exact = O.rel_l2(y, ref)
     print(f"slab320 {fmt}: vs FP64 of the stored values {same:.3e}, "
