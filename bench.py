@@ -532,6 +532,9 @@ def run_batch(args):
                 op = mr.create_op(cfg, S, None, None, _phi2_toep=K)
                 if fmt != "complex64":
                     op.set_kernel_format(fmt, keep_complex64=False)
+                    # waves are packed by the kernels' own bytes: no
+                    # opportunistic blocked copy of the 16-bit codes
+                    op.blocked_copy(False)
                 del K
                 torch.cuda.empty_cache()
                 ops.append(op)

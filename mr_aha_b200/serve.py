@@ -135,11 +135,13 @@ class GPUBackend(Backend):
         free, _ = torch.cuda.mem_get_info()
         cfg.mem_fraction = float(min(0.9, max(1e-4, self.plan_bytes / max(free, 1))))
         op = api.create_op(cfg, req.SEs, req.phi2, req.traj)
-        # the server budgets device memory itself: no opportunistic blocked
-        # kernel copy (it would take memory budgeted for other requests)
         op.blocked_copy(False)
         if self.kernel_format != "complex64":
             op.set_kernel_format(self.kernel_format, keep_complex64=False)
+        # the server budgets device memory itself: no opportunistic blocked
+        # kernel copy of either format (it would take memory budgeted for
+        # other requests)
+        op.blocked_copy(False)
         x = torch.empty_like(req.b)
         solver = op.cg_solver(req.b, x, lam=req.lam, max_iters=req.n_iter, zero_x=True,
                               graph=self.graph)
