@@ -428,7 +428,7 @@ def run_cg(args):
     # a graph and replayed) timed on its own; the median is reported, since
     # the multi-GB allocations of a solve occasionally stall after the kernel
     # copies of a format change were freed and allocated
-    reps = max(3, args.steps // 10)
+    reps = max(5, args.steps // 6)
     res = {}
     x_c64 = None
     y_c64 = op(x)
