@@ -53,6 +53,14 @@ __device__ __forceinline__ float2 mr_i16x2_to_float2(uint32_t w) {
     return make_float2(lo, hi);
 }
 
+// The same for a pair whose sign bits were flipped when it was stored (the
+// int16 blocked copy): one operation fewer per pair.
+__device__ __forceinline__ float2 mr_i16x2b_to_float2(uint32_t t) {
+    const float lo = __uint_as_float(__byte_perm(t, 0x4B000000u, 0x7610)) - 8421376.0f;
+    const float hi = __uint_as_float(__byte_perm(t, 0x4B000000u, 0x7632)) - 8421376.0f;
+    return make_float2(lo, hi);
+}
+
 // A bfloat16 (re, im) pair as two floats (the bf16 bits are the high half
 // of the float's).
 __device__ __forceinline__ float2 mr_bf16x2_to_float2(uint32_t w) {
@@ -105,7 +113,8 @@ __host__ __device__ constexpr int mr_blk16_tri(int L) { return 4 * ((L * (L + 1)
 // 16): `base` points at the location's group 0, group p is 32 groups further
 // per p, and the four codes of a group come from one 16-byte load that the
 // rank-16 walk's consecutive reads share; `s` is the location's scale (the
-// block multiply scales its result once).
+// block multiply scales its result once). int16 codes are stored with their
+// sign bits flipped (mr_i16x2b_to_float2).
 template <int KF>
 struct mr_kload_blk16 {
     const uint4 *base;
@@ -114,7 +123,7 @@ struct mr_kload_blk16 {
         const uint4 q = __ldg(base + (t >> 2) * 32);
         const uint32_t w = (t & 3) == 0 ? q.x : ((t & 3) == 1 ? q.y : ((t & 3) == 2 ? q.z : q.w));
         if constexpr (KF == MR_KF_BF16) return mr_bf16x2_to_float2(w);
-        else return mr_i16x2_to_float2(w);
+        else return mr_i16x2b_to_float2(w);
     }
 };
 
