@@ -175,11 +175,10 @@ __global__ void k_block_kernel_masked(float2 *__restrict__ out, const float2 *__
 // (t, jx, jy, jz) at word ((b ntri4 + t/4) 32 + jx % 32) 4 + t % 4 (block b as
 // in k_block_kernel; pad components zero), and the location's scale at its
 // natural grid index (b 32 + jx % 32), from the reference-layout codes and
-// scales (row = centred grid index). flip = 0x80008000 for int16 codes
-// (stored with their sign bits flipped, zero as 0x80008000), 0 for bf16.
+// scales (row = centred grid index).
 __global__ void k_block_kernel16(uint32_t *__restrict__ out, float *__restrict__ sout,
                                  const uint32_t *__restrict__ K16, const float *__restrict__ scale,
-                                 int Mx, int My, int Mz, int64_t ntri, uint32_t flip) {
+                                 int Mx, int My, int Mz, int64_t ntri) {
     const int64_t vpad = (int64_t)Mx * My * Mz;
     const int64_t ntri4 = (ntri + 3) / 4;
     const int64_t total = vpad * 4 * ntri4;
@@ -196,7 +195,7 @@ __global__ void k_block_kernel16(uint32_t *__restrict__ out, float *__restrict__
         const int64_t row = mr_nat2cent_d(jx, Mx, Mx / 2) +
                             (int64_t)Mx * (mr_nat2cent_d(jy, My, My / 2) +
                                            (int64_t)My * mr_nat2cent_d(jz, Mz, Mz / 2));
-        out[o] = (t < ntri ? K16[t * vpad + row] : 0u) ^ flip;
+        out[o] = t < ntri ? K16[t * vpad + row] : 0u;
         if (t == 0) sout[b * 32 + lane] = scale[row];
     }
 }
@@ -251,7 +250,7 @@ static void op_build_blocked(mr_op op) {
         k_block_kernel16<<<148 * 16, 256, 0, op->stream>>>(
             reinterpret_cast<uint32_t *>(op->K_blk), op->K_blk_scale,
             reinterpret_cast<const uint32_t *>(op->K16), op->K16_scale, g.m[0], g.m[1], g.m[2],
-            ntri, op->kf == MR_KF_I16 ? 0x80008000u : 0u);
+            ntri);
     } else {
         const int pair = op->cfg.L <= 16 ? 1 : 0;
         if (op->cfg.is_masked) {

@@ -26,8 +26,8 @@ Checks, relative L2 (tolerances written in each test):
 2. ``slab320``: a 320 x 320 x 4 stack with L = 16 and 3 coils (the headline
    y and x kernels, blocked copy) against the FP64 oracle, <= 1e-5; the same
    with the copy released (reference layout); the int16 and bf16 kernel
-   formats (their own blocked copies, within FP32 rounding of the reference
-   layout) against the FP64 oracle of the values they store (<= 1e-5) and of the
+   formats (their own blocked copies, bit-identical to the reference layout)
+   against the FP64 oracle of the values they store (<= 1e-5) and of the
    complex64 kernel (int16 <= 1e-4, bf16 <= 5e-3).
 3. ``stack320``: the full headline workload against the reference's own CUDA
    apply (compiled from its sources into ``oracle/_ref`` by
@@ -150,19 +150,13 @@ def test_slab320_16bit_vs_fp64(slab, fmt, tol_exact):
     op.set_kernel_format(fmt)
     try:
         # the 16-bit blocked copy (four codes per 16-byte load), then the
-        # reference layout: the same codes and products; the blocked int16
-        # codes are stored with their sign bits flipped and decoded by one
-        # operation fewer, which the compiler may schedule into a different
-        # FP32 rounding, so the two agree to 1e-6 (bf16: bit-identical)
+        # reference layout: the same codes, decode and products
         y, trace = traced(lambda: host(op(dev(p["x"]))))
         assert f"k_xbdh<N=320,L=16,NC=1,{kf},256,blocked,tma>" in trace, trace
         assert op.blocked_copy(False) is False
         y1, trace1 = traced(lambda: host(op(dev(p["x"]))))
         assert f"k_xbdh<N=320,L=16,NC=1,{kf},256>" in trace1, trace1
-        if fmt == "bf16":
-            np.testing.assert_array_equal(y1, y)
-        else:
-            assert O.rel_l2(y, y1) <= 1e-6, O.rel_l2(y, y1)
+        np.testing.assert_array_equal(y1, y)
     finally:
         op.set_kernel_format("complex64")
     assert op.blocked_copy(True) is True
