@@ -57,7 +57,8 @@ MR_EXPORT int mr_b200_op_profile(mr_op op, const mr_complex *d_x, mr_complex *d_
  * (the 32 frequencies of a warp contiguous per packed component) that the
  * half-length pass 3 reads with constant offsets; it doubles the complex64
  * kernel's footprint (a masked operator's copy covers the whole grid, zero
- * outside the mask). enable = 0 frees the copy (callers that budget device
+ * outside the mask). A 16-bit format (rank <= 16, unmasked) gets its own
+ * blocked copy of the codes and scales when it is set, likewise. enable = 0 frees the copy (callers that budget device
  * memory themselves), enable = 1 builds it if the plan can use it and the
  * device has room. *built (may be NULL) tells whether a copy exists. */
 MR_EXPORT int mr_b200_op_blocked_copy(mr_op op, int enable, int *built);

@@ -642,9 +642,10 @@ class AhAOp:
         return float(ms.value)
 
     def blocked_copy(self, enable: bool) -> bool:
-        """Free (False) or build (True, if it fits) the blocked complex64
-        kernel copy read by pass 3 (``mr_b200_op_blocked_copy``); returns
-        whether a copy exists."""
+        """Free (False) or build (True, if it fits) the blocked copy of the
+        operator's kernel in its current format (complex64, or the 16-bit
+        codes for rank <= 16) read by pass 3 (``mr_b200_op_blocked_copy``);
+        returns whether a copy exists."""
         self._check_open()
         built = ctypes.c_int(0)
         check(lib.mr_b200_op_blocked_copy(self._handle, 1 if enable else 0, ctypes.byref(built)),
