@@ -55,3 +55,21 @@ def test_single_process_helpers():
     b = bench.alg_bytes(wl, 8, 0)
     assert b["apply"] == pytest.approx(97.99e9, rel=1e-3)
     assert bench.alg_bytes(wl, 4, 4)["apply"] == pytest.approx(85.60e9, rel=1e-3)
+
+
+@pytest.mark.parametrize("workload", ["cg320", "batch48", "serve", "toep", "forms"])
+def test_reference_arm_unavailable_line(workload):
+    """The reference arm of the non-headline workloads prints one JSON line
+    saying why it is unavailable and exits 0 (no GPU needed)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = Path(__file__).resolve().parents[1]
+    r = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference",
+                        "--workload", workload], capture_output=True, text=True, timeout=300,
+                       cwd=root)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["unavailable"]
